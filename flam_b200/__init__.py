@@ -1,0 +1,13 @@
+"""flam_b200: FLAM's recursive skeletonization factorization (rskelf) on B200.
+
+Device code: ``flam_b200/csrc`` (sm_100a CUDA), exported through the C ABI of
+``include/flam.h`` as ``flam_b200/libflam_b200.so``.  This package is the
+host-side mirror of the reference's MATLAB entry points.
+"""
+from ._lib import FlamError, lib
+from .api import Factor, hypoct, hypoct_perm, rskelf, rskelf_batched, rskelf_mv, rskelf_sv
+from .registry import Kernel, Proxy
+from . import problems
+
+__all__ = ["FlamError", "lib", "Factor", "hypoct", "hypoct_perm", "rskelf", "rskelf_batched", "rskelf_mv",
+           "rskelf_sv", "Kernel", "Proxy", "problems"]

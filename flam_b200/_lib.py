@@ -1,0 +1,116 @@
+"""ctypes binding of the C ABI in include/flam.h.
+
+The shared library is built in-tree (``flam_b200/libflam_b200.so``) by
+``flam_b200.build``.  There is no fallback: importing a function that needs
+the library raises if it is missing or was built without the device code.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libflam_b200.so")
+
+FLAM_OK = 0
+STATUS = {
+    0: "FLAM_OK", 1: "FLAM_ERR_ARG", 2: "FLAM_ERR_NOT_SPD", 3: "FLAM_ERR_CUDA", 4: "FLAM_ERR_NOMEM",
+    5: "FLAM_ERR_UNSUPPORTED", 6: "FLAM_ERR_TIMEOUT", 7: "FLAM_ERR_ID_CHECK",
+    100: "FLAM_WARN_RRQR_MAXITER", 101: "FLAM_WARN_SINGULAR",
+}
+
+# every symbol include/flam.h declares
+EXPORTS = (
+    "flam_opts_default", "flam_hypoct", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
+    "flam_factor_info", "flam_tree_export", "flam_tree_perm", "flam_factor_sizes", "flam_factor_export",
+    "flam_level_stats", "flam_factor_free", "flam_last_error", "flam_version",
+)
+
+
+class FlamKernel(C.Structure):
+    _fields_ = [("kind", C.c_int), ("scale", C.c_double), ("dval", C.c_double), ("param", C.c_double),
+                ("weights", C.c_void_p), ("normals", C.c_void_p)]
+
+
+class FlamProxy(C.Structure):
+    _fields_ = [("kind", C.c_int), ("p", C.c_int), ("p_rad", C.c_int), ("kernel_kind", C.c_int),
+                ("scale", C.c_double), ("param", C.c_double), ("two_sided", C.c_int)]
+
+
+class FlamOpts(C.Structure):
+    _fields_ = [("lvlmax", C.c_int), ("ext", C.c_void_p), ("Tmax", C.c_double), ("rrqr_iter", C.c_int64),
+                ("symm", C.c_char), ("stop", C.c_int), ("verb", C.c_int), ("stream", C.c_void_p)]
+
+
+class FlamInfo(C.Structure):
+    _fields_ = [("N", C.c_int64), ("ninst", C.c_int), ("d", C.c_int), ("symm", C.c_char), ("nbox", C.c_int64),
+                ("nlvl_max", C.c_int), ("nfactor", C.c_int64), ("nstep", C.c_int), ("bytes", C.c_int64),
+                ("nrem", C.c_int64), ("t_tree", C.c_double), ("t_factor", C.c_double)]
+
+
+class FlamError(RuntimeError):
+    """Error raised with the reference's identifier, e.g. ``FLAM:chksymm:invalidSymm``."""
+
+    def __init__(self, code, msg):
+        self.code = code
+        self.identifier = msg.split(": ", 1)[0] if msg.startswith("FLAM:") else ""
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+
+
+_lib = None
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"flam_b200: CUDA library missing at {LIB_PATH}; run `python -m flam_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    i64p = C.POINTER(C.c_int64)
+    dp = C.POINTER(C.c_double)
+    L.flam_opts_default.argtypes = [C.POINTER(FlamOpts)]
+    L.flam_opts_default.restype = None
+    L.flam_rskelf.argtypes = [P, C.c_int, C.c_int64, C.POINTER(FlamKernel), C.c_double, C.c_double,
+                              C.POINTER(FlamProxy), C.POINTER(FlamOpts), C.POINTER(P)]
+    L.flam_rskelf.restype = C.c_int
+    L.flam_hypoct.argtypes = [P, C.c_int, C.c_int64, C.c_double, C.c_int, P, P, C.POINTER(P)]
+    L.flam_hypoct.restype = C.c_int
+    L.flam_rskelf_batched.argtypes = [C.c_int, P, C.c_int, i64p, C.POINTER(FlamKernel), C.c_double, C.c_double,
+                                      C.POINTER(FlamProxy), C.POINTER(FlamOpts), C.POINTER(P)]
+    L.flam_rskelf_batched.restype = C.c_int
+    for f in ("flam_rskelf_sv", "flam_rskelf_mv"):
+        getattr(L, f).argtypes = [P, P, C.c_int64, C.c_int64, C.c_char]
+        getattr(L, f).restype = C.c_int
+    L.flam_factor_info.argtypes = [P, C.POINTER(FlamInfo)]
+    L.flam_factor_info.restype = C.c_int
+    L.flam_tree_export.argtypes = [P, C.c_int, C.POINTER(C.c_int), i64p, i64p, i64p, i64p, i64p, dp, dp, i64p,
+                                   i64p, i64p, i64p, i64p, i64p, i64p]
+    L.flam_tree_export.restype = C.c_int
+    L.flam_tree_perm.argtypes = [P, C.c_int, i64p]
+    L.flam_tree_perm.restype = C.c_int
+    L.flam_factor_sizes.argtypes = [P, C.c_int, i64p, C.POINTER(C.c_int), i64p, i64p, i64p]
+    L.flam_factor_sizes.restype = C.c_int
+    L.flam_factor_export.argtypes = [P, C.c_int, C.c_int64, i64p, i64p, dp, dp, dp, i64p, dp, dp]
+    L.flam_factor_export.restype = C.c_int
+    L.flam_level_stats.argtypes = [P, C.c_int, C.POINTER(C.c_int), i64p]
+    L.flam_level_stats.restype = C.c_int
+    L.flam_factor_free.argtypes = [P]
+    L.flam_factor_free.restype = None
+    L.flam_last_error.argtypes = []
+    L.flam_last_error.restype = C.c_char_p
+    L.flam_version.argtypes = []
+    L.flam_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(code, allow_warn=True):
+    if code == FLAM_OK:
+        return code
+    msg = lib().flam_last_error().decode()
+    if allow_warn and code >= 100:
+        import warnings
+        warnings.warn(msg)
+        return code
+    raise FlamError(code, msg)

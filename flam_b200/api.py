@@ -1,0 +1,278 @@
+"""MATLAB-signature host API over the C ABI.
+
+    F = rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None)     rskelf/rskelf.m:109
+    Y = rskelf_sv(F, X, trans='n')                                  rskelf/rskelf_sv.m:13
+    Y = rskelf_mv(F, X, trans='n')                                  rskelf/rskelf_mv.m:13
+    T = hypoct(x, occ, lvlmax=inf, ext=None)                        core/hypoct.m:51
+    P = hypoct_perm(T)                                              core/hypoct_perm.m:11
+
+``A`` and ``pxyfun`` are registry descriptors (:class:`flam_b200.Kernel`,
+:class:`flam_b200.Proxy`); a Python callable is rejected with
+``FLAM:gpu:unsupportedHandle`` because the matrix is evaluated on the device.
+Indices are 0-based.  ``X`` may be a NumPy array (host; copied in and out by
+the library) or a CUDA tensor (device pointer, no host copies).
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .registry import Kernel, Proxy
+
+_OPT_KEYS = {"lvlmax", "ext", "Tmax", "rrqr_iter", "symm", "stop", "verb", "stream"}
+
+
+def _c_opts(opts):
+    o = _lib.FlamOpts()
+    _lib.lib().flam_opts_default(C.byref(o))
+    keep = []
+    for k, v in (opts or {}).items():
+        if k not in _OPT_KEYS:
+            continue
+        if k == "lvlmax":
+            o.lvlmax = 0 if (v is None or v == math.inf) else int(v)
+        elif k == "ext":
+            if v is not None and np.size(v):
+                e = np.asfortranarray(v, dtype=np.float64)
+                keep.append(e)
+                o.ext = e.ctypes.data
+        elif k == "Tmax":
+            o.Tmax = float(v)
+        elif k == "rrqr_iter":
+            o.rrqr_iter = -1 if (v is None or v == math.inf) else int(v)
+        elif k == "symm":
+            o.symm = str(v).encode()[:1]
+        elif k == "stop":
+            o.stop = -1 if (v is None or v == math.inf) else int(v)
+        elif k == "verb":
+            o.verb = int(bool(v))
+        elif k == "stream":
+            o.stream = v
+    return o, keep
+
+
+def _is_cuda_tensor(X):
+    return type(X).__module__.startswith("torch") and getattr(X, "is_cuda", False)
+
+
+class Factor:
+    """Handle of a device factorization (the reference's struct ``F``)."""
+
+    def __init__(self, handle, ninst=1, keep=None):
+        self._h = handle
+        self.ninst = ninst
+        self._keep = keep
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().flam_factor_free(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        i = _lib.FlamInfo()
+        _lib.check(_lib.lib().flam_factor_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in i._fields_}
+
+    @property
+    def N(self):
+        return self.info()["N"]
+
+    @property
+    def symm(self):
+        return self.info()["symm"].decode()
+
+    # ---------------------------------------------------------------- exports
+    def tree(self, inst=0):
+        """The reference's hypoct struct (0-based), see core/hypoct.m:15-37."""
+        L = _lib.lib()
+        i64 = C.c_int64
+        nlvl, nbox, nc, nn, npt = C.c_int(), i64(), i64(), i64(), i64()
+        _lib.check(L.flam_tree_export(self._h, inst, C.byref(nlvl), C.byref(nbox), C.byref(nc), C.byref(nn),
+                                      C.byref(npt), *([None] * 11)))
+        d = self.info()["d"]
+        nb = nbox.value
+        lvp = np.zeros(nlvl.value + 1, np.int64)
+        lv = np.zeros(d * nlvl.value)
+        ctr = np.zeros(d * nb)
+        prnt = np.zeros(nb, np.int64)
+        cp = np.zeros(nb + 1, np.int64)
+        ch = np.zeros(max(nc.value, 1), np.int64)
+        npp = np.zeros(nb + 1, np.int64)
+        nbr = np.zeros(max(nn.value, 1), np.int64)
+        xp = np.zeros(nb + 1, np.int64)
+        xi = np.zeros(max(npt.value, 1), np.int64)
+        p64 = lambda a: a.ctypes.data_as(C.POINTER(i64))  # noqa: E731
+        pd = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        _lib.check(L.flam_tree_export(self._h, inst, C.byref(nlvl), C.byref(nbox), C.byref(nc), C.byref(nn),
+                                      C.byref(npt), p64(lvp), pd(lv), pd(ctr), p64(prnt), p64(cp), p64(ch),
+                                      p64(npp), p64(nbr), p64(xp), p64(xi)))
+        return dict(nlvl=nlvl.value, lvp=lvp, l=lv.reshape(nlvl.value, d).T.copy(), ctr=ctr.reshape(nb, d),
+                    prnt=prnt, chld=[ch[cp[b]:cp[b + 1]] for b in range(nb)],
+                    nbor=[nbr[npp[b]:npp[b + 1]] for b in range(nb)], xi=[xi[xp[b]:xp[b + 1]] for b in range(nb)])
+
+    def perm(self, inst=0):
+        n = int(self._inst_sizes()[inst])
+        P = np.zeros(n, np.int64)
+        _lib.check(_lib.lib().flam_tree_perm(self._h, inst, P.ctypes.data_as(C.POINTER(C.c_int64))))
+        return P
+
+    def _inst_sizes(self):
+        sizes = getattr(self, "_sizes", None)
+        if sizes is None:
+            sizes = [sum(len(a) for a in self.tree(i)["xi"]) for i in range(self.ninst)]
+            self._sizes = sizes
+        return sizes
+
+    def factors(self, inst=0):
+        """The reference's ``F`` struct: lvp, factors(i).{sk,rd,T,L,U,p,E,F} (rskelf.m:157-159,249-257)."""
+        L = _lib.lib()
+        i64 = C.c_int64
+        nfac, nlvp = i64(), C.c_int()
+        _lib.check(L.flam_factor_sizes(self._h, inst, C.byref(nfac), C.byref(nlvp), None, None, None))
+        lvp = np.zeros(nlvp.value, np.int64)
+        k = np.zeros(max(nfac.value, 1), np.int64)
+        r = np.zeros(max(nfac.value, 1), np.int64)
+        p64 = lambda a: a.ctypes.data_as(C.POINTER(i64))  # noqa: E731
+        pd = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        _lib.check(L.flam_factor_sizes(self._h, inst, C.byref(nfac), C.byref(nlvp), p64(lvp), p64(k), p64(r)))
+        symm = self.symm
+        out = []
+        for j in range(nfac.value):
+            kk, rr = int(k[j]), int(r[j])
+            sk = np.zeros(max(kk, 1), np.int64)
+            rd = np.zeros(max(rr, 1), np.int64)
+            T = np.zeros((kk, rr), order="F")
+            Lm = np.zeros((rr, rr), order="F")
+            U = np.zeros((rr, rr), order="F")
+            p = np.zeros(max(rr, 1), np.int64)
+            E = np.zeros((kk, rr), order="F")
+            G = np.zeros((rr, kk), order="F")
+            _lib.check(L.flam_factor_export(self._h, inst, j, p64(sk), p64(rd), pd(T), pd(Lm), pd(U), p64(p),
+                                            pd(E), pd(G)))
+            f = dict(sk=sk[:kk], rd=rd[:rr], T=np.ascontiguousarray(T), L=np.ascontiguousarray(Lm), E=np.ascontiguousarray(E))
+            if symm == "p":
+                f.update(U=None, p=None, F=None)
+            else:
+                f.update(U=np.ascontiguousarray(U), p=p[:rr], F=np.ascontiguousarray(G))
+            out.append(f)
+        return dict(N=self._inst_sizes()[inst], lvp=lvp, factors=out, symm=symm)
+
+    def level_stats(self, inst=0):
+        """Rows (lvl, nblk, start npts, end npts) of the opts.verb table (rskelf.m:267-272)."""
+        n = C.c_int()
+        _lib.check(_lib.lib().flam_level_stats(self._h, inst, C.byref(n), None))
+        rows = np.zeros(4 * max(n.value, 1), np.int64)
+        _lib.check(_lib.lib().flam_level_stats(self._h, inst, C.byref(n), rows.ctypes.data_as(C.POINTER(C.c_int64))))
+        return rows[:4 * n.value].reshape(n.value, 4)
+
+    # ---------------------------------------------------------------- apply
+    def sv_(self, X, trans="n"):
+        """In-place solve on a CUDA tensor or Fortran-ordered float64 NumPy array."""
+        return self._apply(X, trans, True)
+
+    def mv_(self, X, trans="n"):
+        return self._apply(X, trans, False)
+
+    def _apply(self, X, trans, solve):
+        L = _lib.lib()
+        fn = L.flam_rskelf_sv if solve else L.flam_rskelf_mv
+        if _is_cuda_tensor(X):
+            import torch
+            if X.dtype != torch.float64:
+                raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: X must be float64")
+            if X.dim() == 1:
+                ptr, ld, nrhs = X.data_ptr(), X.shape[0], 1
+            else:
+                if X.stride(0) != 1:
+                    raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: X must be column-major (X.t().contiguous().t())")
+                ptr, ld, nrhs = X.data_ptr(), X.stride(1), X.shape[1]
+            _lib.check(fn(self._h, C.c_void_p(ptr), ld, nrhs, str(trans).encode()[:1]))
+            return X
+        if not (isinstance(X, np.ndarray) and X.dtype == np.float64 and (X.ndim == 1 or X.flags.f_contiguous)):
+            raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: X must be a float64 Fortran-ordered array")
+        nrhs = 1 if X.ndim == 1 else X.shape[1]
+        _lib.check(fn(self._h, C.c_void_p(X.ctypes.data), X.shape[0], nrhs, str(trans).encode()[:1]))
+        return X
+
+
+def _check_handles(A, pxyfun):
+    if callable(A) and not isinstance(A, Kernel):
+        raise _lib.FlamError(5, "FLAM:gpu:unsupportedHandle: A must be a registry Kernel, not a function handle")
+    if pxyfun is not None and not isinstance(pxyfun, Proxy):
+        raise _lib.FlamError(5, "FLAM:gpu:unsupportedHandle: pxyfun must be a registry Proxy, not a function handle")
+
+
+def rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None):
+    """F = rskelf(A, x, occ, rank_or_tol, pxyfun, opts)   rskelf/rskelf.m:109-309."""
+    _check_handles(A, pxyfun)
+    x = np.asfortranarray(x, dtype=np.float64)
+    d, N = x.shape
+    o, keep = _c_opts(opts)
+    ka = A.c_struct()
+    px = (pxyfun or Proxy("none", 1)).c_struct()
+    h = C.c_void_p()
+    _lib.check(_lib.lib().flam_rskelf(x.ctypes.data, d, N, C.byref(ka), float(occ), float(rank_or_tol), C.byref(px),
+                                      C.byref(o), C.byref(h)))
+    return Factor(h.value, 1)
+
+
+def rskelf_batched(As, xs, occ, rank_or_tol, pxyfun=None, opts=None):
+    """Many independent rskelf problems in one device pipeline (one launch per level step)."""
+    for A in As:
+        _check_handles(A, pxyfun)
+    xs = [np.asfortranarray(x, dtype=np.float64) for x in xs]
+    d = xs[0].shape[0]
+    X = np.asfortranarray(np.concatenate(xs, axis=1))
+    N = np.array([x.shape[1] for x in xs], dtype=np.int64)
+    karr = (_lib.FlamKernel * len(As))(*[A.c_struct() for A in As])
+    o, keep = _c_opts(opts)
+    px = (pxyfun or Proxy("none", 1)).c_struct()
+    h = C.c_void_p()
+    _lib.check(_lib.lib().flam_rskelf_batched(len(As), X.ctypes.data, d, N.ctypes.data_as(C.POINTER(C.c_int64)), karr,
+                                              float(occ), float(rank_or_tol), C.byref(px), C.byref(o), C.byref(h)))
+    F = Factor(h.value, len(As))
+    F._sizes = [int(n) for n in N]
+    return F
+
+
+def rskelf_sv(F, X, trans="n"):
+    """Y = rskelf_sv(F, X, trans): returns a new array (MATLAB value semantics)."""
+    if _is_cuda_tensor(X):
+        Y = X.clone() if X.dim() == 1 else X.t().contiguous().t()
+        return F.sv_(Y, trans)
+    return F.sv_(np.array(X, dtype=np.float64, order="F", copy=True), trans)
+
+
+def rskelf_mv(F, X, trans="n"):
+    """Y = rskelf_mv(F, X, trans): returns a new array."""
+    if _is_cuda_tensor(X):
+        Y = X.clone() if X.dim() == 1 else X.t().contiguous().t()
+        return F.mv_(Y, trans)
+    return F.mv_(np.array(X, dtype=np.float64, order="F", copy=True), trans)
+
+
+def hypoct(x, occ, lvlmax=math.inf, ext=None):
+    """T = hypoct(x, occ, lvlmax, ext), built on the device.   core/hypoct.m:51-171."""
+    x = np.asfortranarray(x, dtype=np.float64)
+    d, N = x.shape
+    e = None if ext is None or np.size(ext) == 0 else np.asfortranarray(ext, dtype=np.float64)
+    lv = 0 if (lvlmax is None or lvlmax == math.inf) else int(lvlmax)
+    if lv < 0 or (lvlmax is not None and lvlmax != math.inf and lvlmax < 1):
+        raise _lib.FlamError(1, "FLAM:hypoct:invalidLvlmax: Maximum tree depth must be at least 1.")
+    h = C.c_void_p()
+    _lib.check(_lib.lib().flam_hypoct(x.ctypes.data, d, N, float(occ), lv, None if e is None else e.ctypes.data,
+                                      None, C.byref(h)))
+    F = Factor(h.value, 1)
+    F._sizes = [N]
+    return F
+
+
+def hypoct_perm(T):
+    """P = hypoct_perm(T) for a handle returned by :func:`hypoct` or :func:`rskelf`."""
+    return T.perm(0)

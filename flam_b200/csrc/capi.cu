@@ -1,0 +1,1303 @@
+// Host driver and C ABI (include/flam.h).
+//
+// The host plans, the device computes.  After the device builds the forest
+// (tree.cu), its arrays are copied to the host once; every factorization step
+// is then planned on the host from the skeleton counts the previous step
+// returned (one small device-to-host copy per step), and executed as four
+// launches: id gathers (slf lists and neighbour candidates), the fused
+// compress kernel, and the elimination kernel.
+//
+// Reference loop being replaced: rskelf/rskelf.m:168-263.  Steps run the
+// boxes of every instance whose level is (its depth - step), leaves first.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/flam.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "scan.cuh"
+#include "tree.cuh"
+
+namespace flam {
+namespace {
+
+thread_local std::string g_err;
+
+struct FlamError : std::runtime_error {
+  flam_status code;
+  FlamError(flam_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(flam_status c, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  throw FlamError(c, buf);
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      fail(e_ == cudaErrorMemoryAllocation ? FLAM_ERR_NOMEM : FLAM_ERR_CUDA, "FLAM:gpu:cuda: %s (%s:%d)", \
+           cudaGetErrorString(e_), __FILE__, __LINE__);                                   \
+  } while (0)
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// Growable device array on one stream.
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  int64_t n = 0, cap = 0;
+  void reserve(int64_t c, cudaStream_t s) {
+    if (c <= cap) return;
+    int64_t nc = std::max<int64_t>(c, cap + cap / 2);
+    nc = std::max<int64_t>(nc, 16);
+    T* q = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void**>(&q), sizeof(T) * nc, s));
+    if (n > 0) CK(cudaMemcpyAsync(q, p, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+    if (p) CK(cudaFreeAsync(p, s));
+    p = q;
+    cap = nc;
+  }
+  void resize(int64_t c, cudaStream_t s) {
+    reserve(c, s);
+    n = c;
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) {
+    n = 0;
+    resize((int64_t)v.size(), s);
+    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  }
+  void release(cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = cap = 0;
+  }
+  int64_t bytes() const { return cap * (int64_t)sizeof(T); }
+};
+
+template <class T>
+std::vector<T> download(const T* p, int64_t n, cudaStream_t s) {
+  std::vector<T> v((size_t)n);
+  if (n > 0) CK(cudaMemcpyAsync(v.data(), p, sizeof(T) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return v;
+}
+
+struct HostFac {
+  int inst, step;
+  int64_t sk_off;
+  int32_t k, r;
+  int64_t fac_off, piv_off;
+};
+
+struct StepDev {
+  DBuf<FacDesc> fac;
+  int nfac = 0, kmax = 0, rmax = 0;
+};
+
+struct LevelStat {
+  int64_t lvl, nblk, nrem1, nrem2;
+};
+
+}  // namespace
+}  // namespace flam
+
+using namespace flam;
+
+struct flam_factor {
+  int dev = 0;
+  cudaStream_t s = nullptr;
+  int d = 0, ninst = 0;
+  int64_t Ntot = 0;
+  char symm = 'n';
+  std::vector<int64_t> inst_off;
+  std::vector<InstParams> iph;
+  // device inputs
+  DBuf<double> x, w, nrm, pxy_pts, pxy_shift;
+  DBuf<InstParams> ip;
+  int npxy = 0;
+  bool has_w = false, has_nrm = false;
+  // tree (host mirror)
+  int64_t nbox = 0;
+  std::vector<int64_t> lvb;  // global depth pointers
+  std::vector<int32_t> prnt, chfirst, nch, depth, binst;
+  std::vector<int64_t> seg_start, seg_len, nbor_ptr;
+  std::vector<int32_t> nbor;
+  std::vector<double> ctr, lsz;
+  std::vector<int> nlvl;     // per instance
+  DBuf<int64_t> hperm;       // hypoct_perm, global positions
+  // factor
+  DBuf<int64_t> ipool;
+  DBuf<double> fpool;
+  DBuf<int32_t> ppool;
+  std::vector<StepDev> steps;
+  std::vector<HostFac> hfac;
+  std::vector<std::vector<int64_t>> inst_fac;     // per instance: indices into hfac
+  std::vector<std::vector<int64_t>> inst_lvp;     // per instance F.lvp
+  std::vector<std::vector<LevelStat>> stats;
+  std::vector<int64_t> rem;  // remaining points per instance
+  double t_tree = 0, t_factor = 0;
+  int64_t warn = 0;
+
+  ~flam_factor() {
+    if (!s && !x.p) return;
+    cudaStream_t st = s;
+    x.release(st);
+    w.release(st);
+    nrm.release(st);
+    pxy_pts.release(st);
+    pxy_shift.release(st);
+    ip.release(st);
+    hperm.release(st);
+    ipool.release(st);
+    fpool.release(st);
+    ppool.release(st);
+    for (auto& q : steps) q.fac.release(st);
+    cudaStreamSynchronize(st);
+  }
+};
+
+namespace flam {
+namespace {
+
+// --------------------------------------------------------------- registry setup
+void proxy_points(const flam_proxy& px, int d, std::vector<double>& pts, std::vector<double>& shift) {
+  const double pi = 3.14159265358979323846;
+  pts.clear();
+  shift.clear();
+  auto fib = [&](int p, double rad, std::vector<double>& out) {
+    out.resize((size_t)p * 3);
+    for (int i = 0; i < p; ++i) {
+      double z = 1.0 - (2.0 * i + 1.0) / p;
+      double rr = std::sqrt(std::max(0.0, 1.0 - z * z));
+      double phi = i * pi * (3.0 - std::sqrt(5.0));
+      out[i * 3 + 0] = rad * rr * std::cos(phi);
+      out[i * 3 + 1] = rad * rr * std::sin(phi);
+      out[i * 3 + 2] = rad * z;
+    }
+  };
+  if (px.kind == FLAM_PROXY_RING) {
+    pts.resize((size_t)px.p * 2);
+    for (int j = 0; j < px.p; ++j) {
+      double t = (j + 1) * 2 * pi / px.p;
+      pts[j * 2] = 1.5 * std::cos(t);
+      pts[j * 2 + 1] = 1.5 * std::sin(t);
+    }
+  } else if (px.kind == FLAM_PROXY_SPHERE) {
+    fib(px.p, 1.5, pts);
+  } else if (px.kind == FLAM_PROXY_ANNULUS) {
+    std::vector<double> base;
+    if (d == 2) {
+      base.resize((size_t)px.p * 2);
+      for (int j = 0; j < px.p; ++j) {
+        double t = (j + 1) * 2 * pi / px.p;
+        base[j * 2] = std::cos(t);
+        base[j * 2 + 1] = std::sin(t);
+      }
+    } else {
+      fib(px.p, 1.0, base);
+    }
+    for (int j = 0; j < px.p; ++j) {
+      double mx = 0;
+      for (int q = 0; q < d; ++q) mx = std::max(mx, std::fabs(base[j * d + q]));
+      for (int q = 0; q < d; ++q) base[j * d + q] /= mx;
+    }
+    const int nr = px.p_rad;
+    const double R = 3.0 / px.param;
+    pts.resize((size_t)px.p * nr * d);
+    shift.resize((size_t)px.p * nr * d);
+    for (int jr = 0; jr < nr; ++jr) {
+      double rad = nr > 1 ? (jr == nr - 1 ? R : jr * (R / (nr - 1))) : 0.0;
+      for (int j = 0; j < px.p; ++j)
+        for (int q = 0; q < d; ++q) {
+          pts[((size_t)jr * px.p + j) * d + q] = base[j * d + q] * rad;
+          shift[((size_t)jr * px.p + j) * d + q] = 1.5 * base[j * d + q];
+        }
+    }
+  }
+}
+
+char chksymm(char c) {
+  c = (char)std::tolower((unsigned char)c);
+  if (c != 'n' && c != 's' && c != 'h' && c != 'p')
+    fail(FLAM_ERR_ARG, "FLAM:chksymm:invalidSymm: Symmetry parameter must be one of 'N', 'S', 'H', or 'P'.");
+  return c;
+}
+
+char chktrans(char c) {
+  c = (char)std::tolower((unsigned char)c);
+  if (c != 'n' && c != 't' && c != 'c')
+    fail(FLAM_ERR_ARG, "FLAM:chktrans:invalidTrans: Transpose parameter must be one of 'N', 'T', or 'C'.");
+  return c;
+}
+
+// --------------------------------------------------------------- tree build (K1, K2)
+void build_tree(flam_factor& F, double occ, const flam_opts& o) {
+  cudaStream_t s = F.s;
+  const int d = F.d, ninst = F.ninst;
+  const int64_t ntot = F.Ntot;
+  const int nl = 1 << d;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s));
+
+  DBuf<int64_t> inst_off_d;
+  inst_off_d.upload(F.inst_off, s);
+
+  // root extents (hypoct.m:65-69)
+  std::vector<double> ext((size_t)ninst * 2 * d);
+  if (o.ext) {
+    for (int i = 0; i < ninst; ++i)
+      for (int q = 0; q < d; ++q) {
+        ext[((size_t)i * d + q) * 2] = o.ext[q];
+        ext[((size_t)i * d + q) * 2 + 1] = o.ext[d + q];
+      }
+  } else {
+    const int nchunk = ninst == 1 ? 64 : 1;
+    DBuf<double> part;
+    part.resize((int64_t)ninst * nchunk * 2 * d, s);
+    tree_extent(F.x.p, d, inst_off_d.p, ninst, nchunk, part.p, s);
+    auto ph = download(part.p, part.n, s);
+    for (int i = 0; i < ninst; ++i)
+      for (int q = 0; q < d; ++q) {
+        double mn = INFINITY, mx = -INFINITY;
+        for (int c = 0; c < nchunk; ++c) {
+          mn = std::min(mn, ph[(((size_t)i * nchunk + c) * 2 * d) + 2 * q]);
+          mx = std::max(mx, ph[(((size_t)i * nchunk + c) * 2 * d) + 2 * q + 1]);
+        }
+        ext[((size_t)i * d + q) * 2] = mn;
+        ext[((size_t)i * d + q) * 2 + 1] = mx;
+      }
+    part.release(s);
+  }
+
+  // device tree arrays
+  DBuf<int64_t> perm, perm2, seg_start, seg_len, nbor_ptr;
+  DBuf<int32_t> pbox, pbox2, prnt, chfirst, nch, depth, binst, keychild, nbor;
+  DBuf<double> ctr, lsz;
+  auto reserve_boxes = [&](int64_t c) {
+    ctr.reserve(c * d, s);
+    lsz.reserve(c * d, s);
+    prnt.reserve(c, s);
+    chfirst.reserve(c, s);
+    nch.reserve(c, s);
+    seg_start.reserve(c, s);
+    seg_len.reserve(c, s);
+    depth.reserve(c, s);
+    binst.reserve(c, s);
+    keychild.reserve(c * 8, s);
+    nbor_ptr.reserve(c + 1, s);
+    ctr.n = lsz.n = c * d;
+    prnt.n = chfirst.n = nch.n = seg_start.n = seg_len.n = depth.n = binst.n = c;
+    keychild.n = c * 8;
+    nbor_ptr.n = c + 1;
+  };
+  {
+    std::vector<int64_t> pv(ntot);
+    std::vector<int32_t> pb(ntot);
+    for (int i = 0; i < ninst; ++i)
+      for (int64_t q = F.inst_off[i]; q < F.inst_off[i + 1]; ++q) {
+        pv[q] = q;
+        pb[q] = i;
+      }
+    perm.upload(pv, s);
+    pbox.upload(pb, s);
+    perm2.resize(ntot, s);
+    pbox2.resize(ntot, s);
+  }
+  std::vector<double> lcur((size_t)ninst * d);
+  {
+    reserve_boxes(std::max<int64_t>(ninst * 4, 64));
+    std::vector<double> c0((size_t)ninst * d), l0((size_t)ninst * d);
+    std::vector<int32_t> z(ninst, 0), one(ninst, 1), mneg(ninst, -1), ids(ninst);
+    std::vector<int64_t> ss(ninst), sl(ninst);
+    for (int i = 0; i < ninst; ++i) {
+      for (int q = 0; q < d; ++q) {
+        const double a = ext[((size_t)i * d + q) * 2], b = ext[((size_t)i * d + q) * 2 + 1];
+        l0[i * d + q] = b - a;
+        c0[i * d + q] = 0.5 * (a + b);
+      }
+      ss[i] = F.inst_off[i];
+      sl[i] = F.inst_off[i + 1] - F.inst_off[i];
+      ids[i] = i;
+    }
+    lcur = l0;
+    CK(cudaMemcpyAsync(ctr.p, c0.data(), sizeof(double) * c0.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(lsz.p, l0.data(), sizeof(double) * l0.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(prnt.p, mneg.data(), sizeof(int32_t) * ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(chfirst.p, mneg.data(), sizeof(int32_t) * ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(nch.p, z.data(), sizeof(int32_t) * ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(depth.p, one.data(), sizeof(int32_t) * ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(binst.p, ids.data(), sizeof(int32_t) * ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(seg_start.p, ss.data(), sizeof(int64_t) * ninst, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(seg_len.p, sl.data(), sizeof(int64_t) * ninst, cudaMemcpyHostToDevice, s));
+  }
+  auto tdev = [&]() {
+    TreeDev t;
+    t.d = d;
+    t.x = F.x.p;
+    t.perm = perm.p;
+    t.pbox = pbox.p;
+    t.ctr = ctr.p;
+    t.lsz = lsz.p;
+    t.prnt = prnt.p;
+    t.chfirst = chfirst.p;
+    t.nch = nch.p;
+    t.seg_start = seg_start.p;
+    t.seg_len = seg_len.p;
+    t.depth = depth.p;
+    t.inst = binst.p;
+    t.keychild = keychild.p;
+    t.nbor_ptr = nbor_ptr.p;
+    t.nbor = nbor.p;
+    return t;
+  };
+
+  const int64_t lvlmax = o.lvlmax <= 0 ? INT64_MAX : o.lvlmax;
+  const int64_t iocc = (int64_t)std::floor(occ);  // xn > occ  <=>  xn > floor(occ) for integer xn
+  std::vector<int64_t> lvb = {0, ninst};
+  DBuf<int32_t> flags, scr32, nchtmp, ldiv_d;
+  DBuf<double> lnew_d;
+  std::vector<int32_t> ldiv(ninst);
+  std::vector<double> lnew((size_t)ninst * d);
+  int D = 1;
+  while (true) {
+    if (D >= lvlmax) break;                                        // hypoct.m:77
+    if (D > 200) fail(FLAM_ERR_ARG, "FLAM:hypoct:depth: tree deeper than 200 levels (duplicate points?)");
+    const int32_t b0 = (int32_t)lvb[D - 1], b1 = (int32_t)lvb[D];
+    for (int i = 0; i < ninst; ++i) {                              // hypoct.m:81-82
+      double mx = -INFINITY;
+      for (int q = 0; q < d; ++q) mx = std::max(mx, lcur[i * d + q]);
+      const double thr = mx / std::sqrt(2.0);
+      int m = 0;
+      for (int q = 0; q < d; ++q) {
+        const bool dv = lcur[i * d + q] >= thr;
+        m |= dv ? (1 << q) : 0;
+        lnew[i * d + q] = dv ? 0.5 * lcur[i * d + q] : lcur[i * d + q];
+      }
+      ldiv[i] = m;
+    }
+    ldiv_d.upload(ldiv, s);
+    lnew_d.upload(lnew, s);
+    TreeDev t = tdev();
+    const int64_t L = (int64_t)nl * (ntot + 1);
+    flags.resize(L + 1, s);
+    scr32.resize(scan_scratch_elems(std::max<int64_t>(L, b1 - b0)) + 1, s);
+    tree_level_flags(t, ntot, b0, b1, iocc, 1, ldiv_d.p, flags.p, nl, s);
+    exclusive_scan<int32_t>(flags.p, flags.p, L, scr32.p, s);
+    nchtmp.resize(b1 - b0 + 1, s);
+    tree_level_count(t, ntot, b0, b1, iocc, 1, flags.p, nl, nchtmp.p, s);
+    exclusive_scan<int32_t>(nchtmp.p, nchtmp.p, b1 - b0, scr32.p, s);
+    int32_t added = 0;
+    CK(cudaMemcpyAsync(&added, nchtmp.p + (b1 - b0), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (added <= 0) break;                                         // hypoct.m:121
+    reserve_boxes((int64_t)b1 + added);
+    t = tdev();
+    tree_level_children(t, ntot, b0, b1, flags.p, nl, nchtmp.p, ldiv_d.p, lnew_d.p, s);
+    tree_level_scatter(t, ntot, b0, b1, iocc, 1, ldiv_d.p, flags.p, nl, perm2.p, pbox2.p, s);
+    std::swap(perm.p, perm2.p);
+    std::swap(pbox.p, pbox2.p);
+    lvb.push_back((int64_t)b1 + added);
+    ++D;
+    lcur = lnew;
+  }
+  const int64_t nbox = lvb.back();
+  const int maxdepth = (int)lvb.size() - 1;
+  // leaves get chfirst = -1 / nch = 0 from their creation; boxes of the last level too.
+
+  // neighbours (hypoct.m:141-170), depth by depth
+  {
+    std::vector<int64_t> z(ninst + 1, 0);
+    CK(cudaMemcpyAsync(nbor_ptr.p, z.data(), sizeof(int64_t) * (ninst + 1), cudaMemcpyHostToDevice, s));
+    DBuf<int64_t> cnt, scr64;
+    int64_t total = 0;
+    nbor.reserve(std::max<int64_t>(nbox * 8, 64), s);
+    for (int Dd = 2; Dd <= maxdepth; ++Dd) {
+      const int32_t b0 = (int32_t)lvb[Dd - 1], b1 = (int32_t)lvb[Dd];
+      const int32_t nb = b1 - b0;
+      cnt.resize(nb + 1, s);
+      scr64.resize(scan_scratch_elems(nb) + 1, s);
+      TreeDev t = tdev();
+      tree_neighbours(t, b0, b1, 0, cnt.p, s);
+      exclusive_scan<int64_t>(cnt.p, cnt.p, nb, scr64.p, s);
+      auto h = download(cnt.p, (int64_t)nb + 1, s);
+      for (auto& v : h) v += total;
+      CK(cudaMemcpyAsync(nbor_ptr.p + b0, h.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, s));
+      total = h[nb];
+      nbor.reserve(total, s);
+      nbor.n = total;
+      t = tdev();
+      tree_neighbours(t, b0, b1, 1, nbor_ptr.p + b0, s);
+    }
+    cnt.release(s);
+    scr64.release(s);
+  }
+
+  // hypoct_perm (hypoct_perm.m:11-39)
+  {
+    DBuf<int64_t> off;
+    off.resize(nbox, s);
+    CK(cudaMemcpyAsync(off.p, F.inst_off.data(), sizeof(int64_t) * ninst, cudaMemcpyHostToDevice, s));
+    TreeDev t = tdev();
+    for (int Dd = 1; Dd < maxdepth; ++Dd) tree_perm_offsets(t, (int32_t)lvb[Dd - 1], (int32_t)lvb[Dd], off.p, s);
+    F.hperm.resize(ntot, s);
+    tree_perm_fill(t, (int32_t)nbox, off.p, F.hperm.p, s);
+    off.release(s);
+  }
+  CK(cudaEventRecord(e1, s));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  F.t_tree = ms * 1e-3;
+  CK(cudaEventDestroy(e0));
+  CK(cudaEventDestroy(e1));
+
+  // host mirror
+  F.nbox = nbox;
+  F.lvb = lvb;
+  F.prnt = download(prnt.p, nbox, s);
+  F.chfirst = download(chfirst.p, nbox, s);
+  F.nch = download(nch.p, nbox, s);
+  F.depth = download(depth.p, nbox, s);
+  F.binst = download(binst.p, nbox, s);
+  F.seg_start = download(seg_start.p, nbox, s);
+  F.seg_len = download(seg_len.p, nbox, s);
+  F.nbor_ptr = download(nbor_ptr.p, nbox + 1, s);
+  F.nbor = download(nbor.p, F.nbor_ptr[nbox], s);
+  F.ctr = download(ctr.p, nbox * d, s);
+  F.lsz = download(lsz.p, nbox * d, s);
+  F.nlvl.assign(ninst, 1);
+  for (int64_t b = 0; b < nbox; ++b) F.nlvl[F.binst[b]] = std::max(F.nlvl[F.binst[b]], (int)F.depth[b]);
+  // the point ids in tree order become the start of the id pool
+  F.ipool.resize(ntot, s);
+  CK(cudaMemcpyAsync(F.ipool.p, perm.p, sizeof(int64_t) * ntot, cudaMemcpyDeviceToDevice, s));
+  for (auto* b : {&perm, &perm2, &seg_start, &seg_len, &nbor_ptr}) b->release(s);
+  for (auto* b : {&pbox, &pbox2, &prnt, &chfirst, &nch, &depth, &binst, &keychild, &nbor, &flags, &scr32,
+                  &nchtmp, &ldiv_d})
+    b->release(s);
+  ctr.release(s);
+  lsz.release(s);
+  lnew_d.release(s);
+  inst_off_d.release(s);
+  CK(cudaStreamSynchronize(s));
+}
+
+// --------------------------------------------------------------- factorization (K3-K7)
+void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
+  cudaStream_t s = F.s;
+  const int ninst = F.ninst;
+  const int64_t nbox = F.nbox;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s));
+
+  // boxes of each (instance, depth), ascending id
+  std::vector<std::vector<std::vector<int32_t>>> byl(ninst);
+  for (int i = 0; i < ninst; ++i) byl[i].resize(F.nlvl[i] + 1);
+  for (int64_t b = 0; b < nbox; ++b) byl[F.binst[b]][F.depth[b]].push_back((int32_t)b);
+  // nonempty (leaf) boxes per level for the verbose table (rskelf.m:146-152)
+  std::vector<std::vector<int64_t>> pblk(ninst);
+  for (int i = 0; i < ninst; ++i) {
+    pblk[i].assign(F.nlvl[i] + 2, 0);
+    for (int L = 1; L <= F.nlvl[i]; ++L) {
+      int64_t c = 0;
+      for (int32_t b : byl[i][L]) c += F.nch[b] == 0;
+      pblk[i][L + 1] = pblk[i][L] + c;
+    }
+  }
+
+  std::vector<int64_t> xoff(nbox), xlen(nbox), Moff(nbox, -1);
+  for (int64_t b = 0; b < nbox; ++b) {
+    const bool leaf = F.nch[b] == 0;
+    xoff[b] = leaf ? F.seg_start[b] : 0;
+    xlen[b] = leaf ? F.seg_len[b] : 0;
+  }
+  F.rem.resize(ninst);
+  for (int i = 0; i < ninst; ++i) F.rem[i] = F.inst_off[i + 1] - F.inst_off[i];
+  F.inst_fac.assign(ninst, {});
+  F.inst_lvp.assign(ninst, {0});
+  F.stats.assign(ninst, {});
+
+  const double rel_tol = std::fmod(rank_or_tol, 1.0);
+  const int kmax = (int)std::min<double>(std::floor(rank_or_tol), 2e9);
+  const int maxsteps = *std::max_element(F.nlvl.begin(), F.nlvl.end());
+  const int64_t stop = o.stop < 0 ? INT64_MAX : o.stop;
+
+  DBuf<int64_t> cpool;
+  DBuf<double> tpool, scratch, mpool[2];
+  DBuf<int32_t> permpool, status;
+  DBuf<CompressTask> ctask;
+  DBuf<ElimTask> etask;
+  DBuf<ChildBlock> chb;
+  DBuf<CopySeg> segs;
+  DBuf<CompressOut> cout;
+  status.resize(1, s);
+  CK(cudaMemsetAsync(status.p, 0, sizeof(int32_t), s));
+  Problem P;
+  P.d = F.d;
+  P.x = F.x.p;
+  P.w = F.has_w ? F.w.p : nullptr;
+  P.nrm = F.has_nrm ? F.nrm.p : nullptr;
+  P.ip = F.ip.p;
+  P.pxy_pts = F.pxy_pts.p;
+  P.pxy_shift = F.pxy_shift.n ? F.pxy_shift.p : nullptr;
+  P.npxy = F.npxy;
+  int cur = 0;  // M pool written this step
+  int64_t fpool_top = 0, ppool_top = 0;
+  const bool prof = std::getenv("FLAM_PROFILE") != nullptr;
+  cudaEvent_t pe[4];
+  if (prof)
+    for (auto& e : pe) CK(cudaEventCreate(&e));
+
+  for (int step = 0; step < maxsteps && step < stop; ++step) {
+    // ---- boxes of this step: level nlvl_i - step of each instance
+    std::vector<int32_t> boxes;
+    std::vector<int> binst_step;
+    for (int i = 0; i < ninst; ++i) {
+      const int L = F.nlvl[i] - step;
+      if (L < 1) continue;
+      for (int32_t b : byl[i][L]) boxes.push_back(b);
+    }
+    if (boxes.empty()) break;
+    const int nb = (int)boxes.size();
+    std::vector<int64_t> rem1 = F.rem;
+    // ---- slf lists: own points (leaf) or children's current xi (rskelf.m:179-181)
+    std::vector<int64_t> slf_off(nb), nslf(nb);
+    std::vector<CopySeg> sg;
+    std::vector<ChildBlock> ch;
+    std::vector<int32_t> ch_first(nb), nchv(nb);
+    int64_t top = F.ipool.n;
+    std::vector<int64_t> pos_in_step(nbox, -1);
+    for (int q = 0; q < nb; ++q) {
+      const int32_t b = boxes[q];
+      pos_in_step[b] = q;
+      slf_off[q] = top;
+      int64_t n = 0;
+      if (F.nch[b] == 0) {
+        sg.push_back(CopySeg{xoff[b], top + n, xlen[b]});
+        n += xlen[b];
+      }
+      ch_first[q] = (int32_t)ch.size();
+      for (int32_t c = F.chfirst[b]; c >= 0 && c < F.chfirst[b] + F.nch[b]; ++c) {
+        ch.push_back(ChildBlock{(int32_t)n, (int32_t)xlen[c], Moff[c]});
+        if (xlen[c] > 0) sg.push_back(CopySeg{xoff[c], top + n, xlen[c]});
+        n += xlen[c];
+      }
+      nchv[q] = (int32_t)ch.size() - ch_first[q];
+      nslf[q] = n;
+      top += n;
+    }
+    F.ipool.reserve(top, s);
+    F.ipool.n = top;
+    // ---- neighbour candidates: current xi of every neighbour (rskelf.m:186)
+    std::vector<CopySeg> cs;
+    std::vector<int64_t> cand_off(nb), ncand(nb);
+    int64_t ctop = 0;
+    for (int q = 0; q < nb; ++q) {
+      const int32_t b = boxes[q];
+      cand_off[q] = ctop;
+      int64_t n = 0;
+      for (int64_t e = F.nbor_ptr[b]; e < F.nbor_ptr[b + 1]; ++e) {
+        const int32_t j = F.nbor[e];
+        int64_t so, sl;
+        if (pos_in_step[j] >= 0) {  // same level: its list after the pull-up (level-synchronous)
+          so = slf_off[pos_in_step[j]];
+          sl = nslf[pos_in_step[j]];
+        } else {                    // coarser leaf: its original points
+          so = xoff[j];
+          sl = xlen[j];
+        }
+        if (sl > 0) cs.push_back(CopySeg{so, ctop + n, sl});
+        n += sl;
+      }
+      ncand[q] = n;
+      ctop += n;
+    }
+    cpool.resize(std::max<int64_t>(ctop, 1), s);
+    // ---- tasks
+    std::vector<CompressTask> ct(nb);
+    int64_t ttop = 0, ptop = 0, stop_s = 0;
+    int nmax_small = 0;
+    for (int q = 0; q < nb; ++q) {
+      const int32_t b = boxes[q];
+      const int i = F.binst[b];
+      CompressTask& t = ct[q];
+      t.slf_off = slf_off[q];
+      t.cand_off = cand_off[q];
+      t.n = (int32_t)nslf[q];
+      t.ncand = (int32_t)ncand[q];
+      t.box = b;
+      t.inst = i;
+      const bool use_proxy = F.depth[b] > 2 && F.iph[i].pkind != P_NONE;   // rskelf.m:203
+      t.flags = use_proxy ? 3 : 0;
+      for (int c = 0; c < kMaxDim; ++c) {
+        t.ctr[c] = c < F.d ? F.ctr[(size_t)b * F.d + c] : 0.0;
+        t.l[c] = c < F.d ? F.lsz[(size_t)b * F.d + c] : 0.0;
+      }
+      t.T_off = ttop;
+      ttop += (nslf[q] * nslf[q]) / 4 + 1;
+      t.perm_off = ptop;
+      ptop += nslf[q];
+      if (nslf[q] > kSmemN) {
+        t.scr_off = stop_s;
+        stop_s += std::max(compress_scratch_doubles((int)nslf[q]), elim_scratch_doubles((int)nslf[q]));
+      } else {
+        t.scr_off = -1;
+        nmax_small = std::max<int>(nmax_small, (int)nslf[q]);
+      }
+    }
+    tpool.resize(std::max<int64_t>(ttop, 1), s);
+    permpool.resize(std::max<int64_t>(ptop, 1), s);
+    scratch.resize(std::max<int64_t>(stop_s, 1), s);
+    segs.upload(sg, s);
+    launch_gather_ids(F.ipool.p, F.ipool.p, segs.p, (int)sg.size(), s);
+    DBuf<CopySeg> csegs;
+    csegs.upload(cs, s);
+    launch_gather_ids(F.ipool.p, cpool.p, csegs.p, (int)cs.size(), s);
+    ctask.upload(ct, s);
+    cout.resize(nb, s);
+    CompressArgs ca;
+    ca.P = P;
+    ca.tasks = ctask.p;
+    ca.ipool = F.ipool.p;
+    ca.cpool = cpool.p;
+    ca.tpool = tpool.p;
+    ca.permpool = permpool.p;
+    ca.scratch = scratch.p;
+    ca.out = cout.p;
+    ca.rel_tol = rel_tol;
+    ca.kmax = kmax;
+    ca.symm_n = F.symm == 'n' ? 1 : 0;
+    ca.Tmax = o.Tmax;
+    ca.rrqr_iter = o.rrqr_iter;
+    if (prof) CK(cudaEventRecord(pe[0], s));
+    launch_compress(ca, nb, compress_smem_bytes(nmax_small), s);
+    CK(cudaGetLastError());
+    if (prof) CK(cudaEventRecord(pe[1], s));
+    auto co = download(cout.p, nb, s);
+    csegs.release(s);
+
+    // ---- elimination plan
+    std::vector<ElimTask> et(nb);
+    std::vector<FacDesc> fd;
+    int64_t mtop = 0;
+    int kmx = 0, rmx = 0, nmax_e = 0;
+    const bool chol = F.symm == 'p';
+    for (int q = 0; q < nb; ++q) {
+      const int32_t b = boxes[q];
+      const int n = (int)nslf[q], k = co[q].k, r = n - k;
+      if (co[q].status & ST_RRQR_CAP) F.warn |= 1;
+      ElimTask& t = et[q];
+      t.slf_off = slf_off[q];
+      t.T_off = ct[q].T_off;
+      t.perm_off = ct[q].perm_off;
+      t.n = n;
+      t.k = k;
+      t.inst = F.binst[b];
+      t.ch_first = ch_first[q];
+      t.nch = nchv[q];
+      t.scr_off = ct[q].scr_off;
+      if (n <= kSmemN) nmax_e = std::max(nmax_e, n);
+      t.M_out = mtop;
+      mtop += r > 0 ? (int64_t)k * k : (int64_t)n * n;
+      if (r > 0) {
+        const int64_t kr = (int64_t)k * r, rr = (int64_t)r * r;
+        t.fac_off = fpool_top;
+        t.piv_off = ppool_top;
+        FacDesc f;
+        f.sk_off = slf_off[q];
+        f.T_off = fpool_top;
+        f.LU_off = fpool_top + kr;
+        f.E_off = fpool_top + kr + rr;
+        f.G_off = fpool_top + 2 * kr + rr;
+        f.piv_off = ppool_top;
+        f.k = k;
+        f.r = r;
+        fd.push_back(f);
+        HostFac h{t.inst, step, slf_off[q], k, r, fpool_top, ppool_top};
+        F.inst_fac[t.inst].push_back((int64_t)F.hfac.size());
+        F.hfac.push_back(h);
+        fpool_top += 2 * kr + rr + (chol ? 0 : kr);
+        ppool_top += chol ? 0 : r;
+        kmx = std::max(kmx, k);
+        rmx = std::max(rmx, r);
+        F.rem[t.inst] -= r;
+      } else {
+        t.fac_off = -1;
+        t.piv_off = -1;
+      }
+    }
+    F.fpool.reserve(std::max<int64_t>(fpool_top, 1), s);
+    F.fpool.n = fpool_top;
+    F.ppool.reserve(std::max<int64_t>(ppool_top, 1), s);
+    F.ppool.n = ppool_top;
+    mpool[cur].resize(std::max<int64_t>(mtop, 1), s);
+    etask.upload(et, s);
+    chb.upload(ch, s);
+    ElimArgs ea;
+    ea.P = P;
+    ea.tasks = etask.p;
+    ea.children = chb.p;
+    ea.ipool = F.ipool.p;
+    ea.tpool = tpool.p;
+    ea.permpool = permpool.p;
+    ea.m_in = mpool[cur ^ 1].p;
+    ea.m_out = mpool[cur].p;
+    ea.fpool = F.fpool.p;
+    ea.ppool = F.ppool.p;
+    ea.scratch = scratch.p;
+    ea.status = status.p;
+    ea.symm = F.symm;
+    if (prof) CK(cudaEventRecord(pe[2], s));
+    launch_eliminate(ea, nb, elim_smem_bytes(nmax_e), s);
+    CK(cudaGetLastError());
+    if (prof) {
+      CK(cudaEventRecord(pe[3], s));
+      CK(cudaEventSynchronize(pe[3]));
+      float tc = 0, tel = 0;
+      CK(cudaEventElapsedTime(&tc, pe[0], pe[1]));
+      CK(cudaEventElapsedTime(&tel, pe[2], pe[3]));
+      int64_t nmx = 0, cmx = 0, mmx = 0, kmx2 = 0, nit = 0, nbig = 0;
+      for (int q = 0; q < nb; ++q) {
+        nmx = std::max<int64_t>(nmx, nslf[q]);
+        cmx = std::max<int64_t>(cmx, ncand[q]);
+        mmx = std::max<int64_t>(mmx, co[q].m);
+        kmx2 = std::max<int64_t>(kmx2, co[q].k);
+        nit += co[q].niter;
+        nbig += nslf[q] > kSmemN;
+      }
+      fprintf(stderr, "[flam] step %2d boxes %6d nmax %5lld big %4lld candmax %6lld mmax %6lld kmax %4lld rrqr %5lld"
+              "  compress %8.3f ms  elim %8.3f ms\n", step, nb, (long long)nmx, (long long)nbig, (long long)cmx,
+              (long long)mmx, (long long)kmx2, (long long)nit, tc, tel);
+    }
+    StepDev sd;
+    sd.fac.upload(fd, s);
+    sd.nfac = (int)fd.size();
+    sd.kmax = kmx;
+    sd.rmax = rmx;
+    F.steps.push_back(std::move(sd));
+    // ---- host state for the next step (rskelf.m:245-261)
+    for (int q = 0; q < nb; ++q) {
+      const int32_t b = boxes[q];
+      const int n = (int)nslf[q], k = co[q].k;
+      xoff[b] = slf_off[q];
+      xlen[b] = (n - k > 0) ? k : n;
+      Moff[b] = et[q].M_out;
+    }
+    // per instance: F.lvp and the verbose table row
+    std::vector<int> seen(ninst, 0);
+    for (int q = 0; q < nb; ++q) seen[F.binst[boxes[q]]] = 1;
+    for (int i = 0; i < ninst; ++i) {
+      if (!seen[i]) continue;
+      F.inst_lvp[i].push_back((int64_t)F.inst_fac[i].size());
+      const int L = F.nlvl[i] - step;
+      const int64_t nblk = pblk[i][L] + (int64_t)byl[i][L].size();
+      F.stats[i].push_back(LevelStat{L, nblk, rem1[i], F.rem[i]});
+    }
+    cur ^= 1;
+  }
+  // make sure the pools reflect their sizes
+  int32_t st = 0;
+  CK(cudaMemcpyAsync(&st, status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(e1, s));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  F.t_factor = ms * 1e-3;
+  CK(cudaEventDestroy(e0));
+  CK(cudaEventDestroy(e1));
+  for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1]}) b->release(s);
+  cpool.release(s);
+  permpool.release(s);
+  status.release(s);
+  ctask.release(s);
+  etask.release(s);
+  chb.release(s);
+  segs.release(s);
+  cout.release(s);
+  CK(cudaStreamSynchronize(s));
+  if (st & ST_NOT_SPD)
+    fail(FLAM_ERR_NOT_SPD, "FLAM:rskelf:notPosDef: a redundant block is not positive definite (chol failed)");
+  if (st & ST_SINGULAR) F.warn |= 2;
+}
+
+void print_table(const flam_factor& F) {
+  if (F.stats.empty()) return;
+  printf("%s\n", std::string(69, '-').c_str());
+  printf("%3s | %6s | %19s | %19s | %10s\n", "lvl", "nblk", "start/end npts", "start/end npts/blk", "time (s)");
+  printf("%s\n", std::string(69, '-').c_str());
+  printf("%3s | %63.2e\n", "t", F.t_tree);
+  for (const auto& r : F.stats[0])
+    printf("%3lld | %6lld | %8lld | %8lld | %8.2f | %8.2f | %10s\n", (long long)r.lvl, (long long)r.nblk,
+           (long long)r.nrem1, (long long)r.nrem2, (double)r.nrem1 / r.nblk, (double)r.nrem2 / r.nblk, "-");
+  printf("%s\n", std::string(69, '-').c_str());
+  fflush(stdout);
+}
+
+flam_status create(int ninst, const double* x, int d, const int64_t* N, const flam_kernel* A, double occ,
+                   double rank_or_tol, const flam_proxy* pxy, const flam_opts* opts_in, flam_factor** out) {
+  if (!out) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: output handle pointer is NULL");
+  *out = nullptr;
+  flam_opts o;
+  flam_opts_default(&o);
+  if (opts_in) o = *opts_in;
+  if (ninst < 1) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: need at least one instance");
+  if (d < 1 || d > kMaxDim) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidDim: dimension must be 1, 2 or 3");
+  if (!x || !A || !N) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: x, N and A must not be NULL");
+  if (!(occ >= 0)) fail(FLAM_ERR_ARG, "FLAM:hypoct:invalidOcc: Leaf occupancy must be nonnegative.");
+  if (!(rank_or_tol >= 0)) fail(FLAM_ERR_ARG, "FLAM:id:invalidRankOrTol: Rank or tolerance must be nonnegative.");
+  if (!(o.Tmax >= 1)) fail(FLAM_ERR_ARG, "FLAM:id:invalidTmax: Interpolation matrix entry bound must be >= 1.");
+  const char symm = chksymm(o.symm);
+  if (symm == 'h')
+    fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h' (LDL) is not available on the device path");
+  flam_proxy px{};
+  px.kind = FLAM_PROXY_NONE;
+  if (pxy) px = *pxy;
+  if (px.kind < 0 || px.kind > 3) fail(FLAM_ERR_ARG, "FLAM:gpu:unsupportedProxy: unknown proxy kind %d", px.kind);
+  if (px.kind == FLAM_PROXY_NONE)
+    fail(FLAM_ERR_UNSUPPORTED,
+         "FLAM:gpu:unsupportedHandle: rskelf without a proxy (global compression) is not available on the device");
+  if (px.kind == FLAM_PROXY_RING && d != 2) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: ring proxy needs d = 2");
+  if (px.kind == FLAM_PROXY_SPHERE && d != 3) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: sphere proxy needs d = 3");
+  if (px.p < 1) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: proxy needs p >= 1 points");
+  if (px.kind == FLAM_PROXY_ANNULUS && (px.p_rad < 1 || !(px.param > 0)))
+    fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: annulus proxy needs p_rad >= 1 and param > 0");
+  if (px.kernel_kind < 0 || px.kernel_kind > 4 || px.kernel_kind == FLAM_KERNEL_LAPLACE2D_DL)
+    fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: proxy kernel must be a single-layer registry kernel");
+  bool any_w = false, any_n = false;
+  for (int i = 0; i < ninst; ++i) {
+    if (N[i] < 1) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: every instance needs N >= 1");
+    if (A[i].kind < 0 || A[i].kind > 4) fail(FLAM_ERR_ARG, "FLAM:gpu:unsupportedKernel: unknown kernel %d", A[i].kind);
+    if (A[i].kind == FLAM_KERNEL_LAPLACE2D_DL && (!A[i].normals || d != 2))
+      fail(FLAM_ERR_ARG, "FLAM:gpu:invalidKernel: the 2D double layer needs d = 2 and normals");
+    any_w |= A[i].weights != nullptr;
+    any_n |= A[i].normals != nullptr;
+  }
+  if (any_w)
+    for (int i = 0; i < ninst; ++i)
+      if (!A[i].weights) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidKernel: weights must be given for all instances or none");
+
+  std::unique_ptr<flam_factor> F(new flam_factor());
+  CK(cudaGetDevice(&F->dev));
+  F->s = (cudaStream_t)o.stream;
+  F->d = d;
+  F->ninst = ninst;
+  F->symm = symm;
+  F->inst_off.assign(ninst + 1, 0);
+  for (int i = 0; i < ninst; ++i) F->inst_off[i + 1] = F->inst_off[i] + N[i];
+  F->Ntot = F->inst_off[ninst];
+  cudaStream_t s = F->s;
+  const int64_t ntot = F->Ntot;
+  // inputs to the device
+  F->x.resize(ntot * d, s);
+  CK(cudaMemcpyAsync(F->x.p, x, sizeof(double) * ntot * d, cudaMemcpyDefault, s));
+  if (any_w) {
+    F->has_w = true;
+    F->w.resize(ntot, s);
+    for (int i = 0; i < ninst; ++i)
+      CK(cudaMemcpyAsync(F->w.p + F->inst_off[i], A[i].weights, sizeof(double) * N[i], cudaMemcpyDefault, s));
+  }
+  if (any_n) {
+    F->has_nrm = true;
+    F->nrm.resize(ntot * d, s);
+    CK(cudaMemsetAsync(F->nrm.p, 0, sizeof(double) * ntot * d, s));
+    for (int i = 0; i < ninst; ++i)
+      if (A[i].normals)
+        CK(cudaMemcpyAsync(F->nrm.p + F->inst_off[i] * d, A[i].normals, sizeof(double) * N[i] * d,
+                           cudaMemcpyDefault, s));
+  }
+  F->iph.resize(ninst);
+  for (int i = 0; i < ninst; ++i) {
+    InstParams& p = F->iph[i];
+    p.pt_off = F->inst_off[i];
+    p.N = N[i];
+    p.kind = A[i].kind;
+    p.has_w = A[i].weights ? 1 : 0;
+    p.has_nrm = A[i].normals ? 1 : 0;
+    p.scale = A[i].scale;
+    p.dval = A[i].dval;
+    p.param = A[i].param;
+    p.wbar = 1.0;
+    if (A[i].weights) {
+      // mean column weight, summed on the host from the caller's array (host or device)
+      std::vector<double> wv(N[i]);
+      CK(cudaMemcpyAsync(wv.data(), A[i].weights, sizeof(double) * N[i], cudaMemcpyDefault, s));
+      CK(cudaStreamSynchronize(s));
+      double acc = 0;
+      for (double v : wv) acc += v;
+      p.wbar = acc / N[i];
+    }
+    p.pkind = px.kind;
+    p.pkernel = px.kernel_kind;
+    p.pscale = px.scale;
+    p.pparam = px.param;
+    p.two_sided = px.two_sided && A[i].weights ? 1 : 0;
+  }
+  F->ip.upload(F->iph, s);
+  std::vector<double> pts, shift;
+  proxy_points(px, d, pts, shift);
+  F->npxy = (int)(pts.size() / d);
+  F->pxy_pts.upload(pts, s);
+  if (!shift.empty()) F->pxy_shift.upload(shift, s);
+
+  build_tree(*F, occ, o);
+  factorize(*F, rank_or_tol, o);
+  if (o.verb) print_table(*F);
+  *out = F.release();
+  if ((*out)->warn & 1) {
+    g_err = "FLAM:id:maxIterCount: Maximum number of RRQR iterations reached.";
+    return FLAM_WARN_RRQR_MAXITER;
+  }
+  if ((*out)->warn & 2) {
+    g_err = "FLAM:rskelf:singular: an LU pivot of a redundant block was exactly zero";
+    return FLAM_WARN_SINGULAR;
+  }
+  return FLAM_OK;
+}
+
+flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans, bool solve) {
+  if (!F) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: NULL factor");
+  trans = chktrans(trans);
+  if (nrhs < 0 || ldx < F->Ntot) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad X dimensions");
+  if (nrhs == 0 || F->Ntot == 0) return FLAM_OK;
+  if (!X) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: X is NULL");
+  cudaStream_t s = F->s;
+  const int t = trans == 'n' ? 0 : 1;   // real data: 't' == 'c' (rskelf_sv.m:22)
+  const int64_t N = F->Ntot;
+  const bool dev = is_device_ptr(X);
+  double* Xd = X;
+  int64_t ld = ldx;
+  DBuf<double> tmp, W;
+  if (!dev) {
+    tmp.resize(N * nrhs, s);
+    CK(cudaMemcpy2DAsync(tmp.p, sizeof(double) * N, X, sizeof(double) * ldx, sizeof(double) * N, nrhs,
+                         cudaMemcpyHostToDevice, s));
+    Xd = tmp.p;
+    ld = N;
+  }
+  W.resize(N * nrhs, s);
+  launch_to_pointmajor(Xd, ld, N, (int)nrhs, W.p, s);
+  SweepArgs a;
+  a.ipool = F->ipool.p;
+  a.fpool = F->fpool.p;
+  a.ppool = F->ppool.p;
+  a.X = W.p;
+  a.ldx = nrhs;
+  a.nrhs = (int)nrhs;
+  a.trans = t;
+  a.symm = F->symm;
+  const int ns = (int)F->steps.size();
+  a.op = solve ? 0 : 2;
+  for (int q = 0; q < ns; ++q) {
+    a.fac = F->steps[q].fac.p;
+    launch_sweep(a, F->steps[q].nfac, F->steps[q].kmax, F->steps[q].rmax, s);
+  }
+  a.op = solve ? 1 : 3;
+  for (int q = ns - 1; q >= 0; --q) {
+    a.fac = F->steps[q].fac.p;
+    launch_sweep(a, F->steps[q].nfac, F->steps[q].kmax, F->steps[q].rmax, s);
+  }
+  CK(cudaGetLastError());
+  launch_from_pointmajor(W.p, N, (int)nrhs, Xd, ld, s);
+  if (!dev)
+    CK(cudaMemcpy2DAsync(X, sizeof(double) * ldx, tmp.p, sizeof(double) * N, sizeof(double) * N, nrhs,
+                         cudaMemcpyDeviceToHost, s));
+  W.release(s);
+  tmp.release(s);
+  if (!dev) CK(cudaStreamSynchronize(s));
+  return FLAM_OK;
+}
+
+template <class Fn>
+flam_status guard(Fn&& fn) {
+  try {
+    return fn();
+  } catch (const FlamError& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_err = std::string("FLAM:gpu:internal: ") + e.what();
+    return FLAM_ERR_CUDA;
+  }
+}
+
+}  // namespace
+}  // namespace flam
+
+extern "C" {
+
+void flam_opts_default(flam_opts* o) {
+  if (!o) return;
+  o->lvlmax = 0;
+  o->ext = nullptr;
+  o->Tmax = 2.0;
+  o->rrqr_iter = -1;
+  o->symm = 'n';
+  o->stop = -1;
+  o->verb = 0;
+  o->stream = nullptr;
+}
+
+flam_status flam_rskelf(const double* x, int d, int64_t N, const flam_kernel* A, double occ, double rank_or_tol,
+                        const flam_proxy* pxy, const flam_opts* opts, flam_factor** F) {
+  return guard([&] { return create(1, x, d, &N, A, occ, rank_or_tol, pxy, opts, F); });
+}
+
+flam_status flam_hypoct(const double* x, int d, int64_t N, double occ, int lvlmax, const double* ext, void* stream,
+                        flam_factor** T) {
+  return guard([&] {
+    if (!T) fail(FLAM_ERR_ARG, "FLAM:hypoct:invalidArg: output handle pointer is NULL");
+    *T = nullptr;
+    if (!x || N < 1 || d < 1 || d > kMaxDim) fail(FLAM_ERR_ARG, "FLAM:hypoct:invalidArg: bad points");
+    if (!(occ >= 0)) fail(FLAM_ERR_ARG, "FLAM:hypoct:invalidOcc: Leaf occupancy must be nonnegative.");
+    std::unique_ptr<flam_factor> F(new flam_factor());
+    CK(cudaGetDevice(&F->dev));
+    F->s = (cudaStream_t)stream;
+    F->d = d;
+    F->ninst = 1;
+    F->inst_off = {0, N};
+    F->Ntot = N;
+    F->x.resize(N * d, F->s);
+    CK(cudaMemcpyAsync(F->x.p, x, sizeof(double) * N * d, cudaMemcpyDefault, F->s));
+    flam_opts o;
+    flam_opts_default(&o);
+    o.lvlmax = lvlmax;
+    o.ext = ext;
+    build_tree(*F, occ, o);
+    F->rem.assign(1, N);
+    F->inst_fac.assign(1, {});
+    F->inst_lvp.assign(1, {0});
+    F->stats.assign(1, {});
+    *T = F.release();
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_rskelf_batched(int ninst, const double* x, int d, const int64_t* N, const flam_kernel* A,
+                                double occ, double rank_or_tol, const flam_proxy* pxy, const flam_opts* opts,
+                                flam_factor** F) {
+  return guard([&] { return create(ninst, x, d, N, A, occ, rank_or_tol, pxy, opts, F); });
+}
+
+flam_status flam_rskelf_sv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {
+  return guard([&] { return apply(F, X, ldx, nrhs, trans, true); });
+}
+
+flam_status flam_rskelf_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {
+  return guard([&] { return apply(F, X, ldx, nrhs, trans, false); });
+}
+
+flam_status flam_factor_info(const flam_factor* F, flam_info* info) {
+  return guard([&] {
+    if (!F || !info) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: NULL argument");
+    info->N = F->Ntot;
+    info->ninst = F->ninst;
+    info->d = F->d;
+    info->symm = F->symm;
+    info->nbox = F->nbox;
+    info->nlvl_max = F->nlvl.empty() ? 0 : *std::max_element(F->nlvl.begin(), F->nlvl.end());
+    info->nfactor = (int64_t)F->hfac.size();
+    info->nstep = (int)F->steps.size();
+    int64_t b = F->ipool.bytes() + F->fpool.bytes() + F->ppool.bytes() + F->x.bytes() + F->hperm.bytes();
+    for (auto& q : F->steps) b += q.fac.bytes();
+    info->bytes = b;
+    int64_t r = 0;
+    for (auto v : F->rem) r += v;
+    info->nrem = r;
+    info->t_tree = F->t_tree;
+    info->t_factor = F->t_factor;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_tree_export(const flam_factor* F, int inst, int* nlvl, int64_t* nbox_o, int64_t* nchld_tot,
+                             int64_t* nnbor_tot, int64_t* npts_tot, int64_t* lvp, double* l, double* ctr,
+                             int64_t* prnt, int64_t* chld_ptr, int64_t* chld, int64_t* nbor_ptr, int64_t* nbor,
+                             int64_t* xi_ptr, int64_t* xi) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad instance");
+    const int d = F->d;
+    std::vector<int64_t> loc(F->nbox, -1), boxes;
+    for (int64_t b = 0; b < F->nbox; ++b)
+      if (F->binst[b] == inst) {
+        loc[b] = (int64_t)boxes.size();
+        boxes.push_back(b);
+      }
+    const int64_t nb = (int64_t)boxes.size();
+    int64_t nc = 0, nn = 0, np = 0;
+    for (int64_t b : boxes) {
+      nc += F->nch[b];
+      nn += F->nbor_ptr[b + 1] - F->nbor_ptr[b];
+      np += F->nch[b] == 0 ? F->seg_len[b] : 0;
+    }
+    if (nlvl) *nlvl = F->nlvl[inst];
+    if (nbox_o) *nbox_o = nb;
+    if (nchld_tot) *nchld_tot = nc;
+    if (nnbor_tot) *nnbor_tot = nn;
+    if (npts_tot) *npts_tot = np;
+    const int L = F->nlvl[inst];
+    if (lvp) {
+      lvp[0] = 0;
+      for (int q = 1; q <= L; ++q) {
+        int64_t c = 0;
+        for (int64_t b : boxes) c += F->depth[b] <= q;
+        lvp[q] = c;
+      }
+    }
+    if (l)
+      for (int q = 1; q <= L; ++q)
+        for (int64_t b : boxes)
+          if (F->depth[b] == q) {
+            for (int c = 0; c < d; ++c) l[(q - 1) * d + c] = F->lsz[b * d + c];
+            break;
+          }
+    std::vector<int64_t> ptsv;
+    if (xi) {
+      std::vector<int64_t> all = download(F->ipool.p, F->Ntot, F->s);
+      ptsv.swap(all);
+    }
+    int64_t oc = 0, on = 0, op = 0;
+    for (int64_t q = 0; q < nb; ++q) {
+      const int64_t b = boxes[q];
+      if (ctr)
+        for (int c = 0; c < d; ++c) ctr[q * d + c] = F->ctr[b * d + c];
+      if (prnt) prnt[q] = F->prnt[b] < 0 ? -1 : loc[F->prnt[b]];
+      if (chld_ptr) chld_ptr[q] = oc;
+      for (int32_t c = 0; c < F->nch[b]; ++c) {
+        if (chld) chld[oc] = loc[F->chfirst[b] + c];
+        ++oc;
+      }
+      if (nbor_ptr) nbor_ptr[q] = on;
+      for (int64_t e = F->nbor_ptr[b]; e < F->nbor_ptr[b + 1]; ++e) {
+        if (nbor) nbor[on] = loc[F->nbor[e]];
+        ++on;
+      }
+      if (xi_ptr) xi_ptr[q] = op;
+      if (F->nch[b] == 0) {
+        for (int64_t e = 0; e < F->seg_len[b]; ++e) {
+          if (xi) xi[op] = ptsv[F->seg_start[b] + e] - F->inst_off[inst];
+          ++op;
+        }
+      }
+    }
+    if (chld_ptr) chld_ptr[nb] = oc;
+    if (nbor_ptr) nbor_ptr[nb] = on;
+    if (xi_ptr) xi_ptr[nb] = op;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_tree_perm(const flam_factor* F, int inst, int64_t* P) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst || !P) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad argument");
+    const int64_t a = F->inst_off[inst], n = F->inst_off[inst + 1] - a;
+    auto v = download(F->hperm.p + a, n, F->s);
+    for (int64_t q = 0; q < n; ++q) P[q] = v[q] - a;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_factor_sizes(const flam_factor* F, int inst, int64_t* nfac, int* nlvp, int64_t* lvp, int64_t* k,
+                              int64_t* r) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad instance");
+    const auto& fl = F->inst_fac[inst];
+    if (nfac) *nfac = (int64_t)fl.size();
+    if (nlvp) *nlvp = (int)F->inst_lvp[inst].size();
+    if (lvp)
+      for (size_t q = 0; q < F->inst_lvp[inst].size(); ++q) lvp[q] = F->inst_lvp[inst][q];
+    for (size_t q = 0; q < fl.size(); ++q) {
+      if (k) k[q] = F->hfac[fl[q]].k;
+      if (r) r[q] = F->hfac[fl[q]].r;
+    }
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_factor_export(const flam_factor* F, int inst, int64_t j, int64_t* sk, int64_t* rd, double* T,
+                               double* L, double* U, int64_t* p, double* E, double* G) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad instance");
+    const auto& fl = F->inst_fac[inst];
+    if (j < 0 || j >= (int64_t)fl.size()) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: factor index out of range");
+    const HostFac& h = F->hfac[fl[j]];
+    const int64_t k = h.k, r = h.r, kr = k * r, rr = r * r;
+    const bool chol = F->symm == 'p';
+    auto ids = download(F->ipool.p + h.sk_off, k + r, F->s);
+    const int64_t a = F->inst_off[inst];
+    if (sk)
+      for (int64_t q = 0; q < k; ++q) sk[q] = ids[q] - a;
+    if (rd)
+      for (int64_t q = 0; q < r; ++q) rd[q] = ids[k + q] - a;
+    auto fv = download(F->fpool.p + h.fac_off, 2 * kr + rr + (chol ? 0 : kr), F->s);
+    if (T) std::copy(fv.begin(), fv.begin() + kr, T);
+    const double* LU = fv.data() + kr;
+    for (int64_t c = 0; c < r; ++c)
+      for (int64_t q = 0; q < r; ++q) {
+        const double v = LU[q + c * r];
+        if (chol) {
+          if (L) L[q + c * r] = q >= c ? v : 0.0;
+        } else {
+          if (L) L[q + c * r] = q > c ? v : (q == c ? 1.0 : 0.0);
+          if (U) U[q + c * r] = q <= c ? v : 0.0;
+        }
+      }
+    if (E) std::copy(fv.begin() + kr + rr, fv.begin() + 2 * kr + rr, E);
+    if (!chol) {
+      if (G) std::copy(fv.begin() + 2 * kr + rr, fv.begin() + 3 * kr + rr, G);
+      if (p) {
+        auto pv = download(F->ppool.p + h.piv_off, r, F->s);
+        for (int64_t q = 0; q < r; ++q) p[q] = pv[q];
+      }
+    }
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_level_stats(const flam_factor* F, int inst, int* nrows, int64_t* rows) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad instance");
+    const auto& st = F->stats[inst];
+    if (nrows) *nrows = (int)st.size();
+    if (rows)
+      for (size_t q = 0; q < st.size(); ++q) {
+        rows[q * 4 + 0] = st[q].lvl;
+        rows[q * 4 + 1] = st[q].nblk;
+        rows[q * 4 + 2] = st[q].nrem1;
+        rows[q * 4 + 3] = st[q].nrem2;
+      }
+    return FLAM_OK;
+  });
+}
+
+void flam_factor_free(flam_factor* F) { delete F; }
+
+const char* flam_last_error(void) { return g_err.c_str(); }
+
+const char* flam_version(void) { return "flam_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

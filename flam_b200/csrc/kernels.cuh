@@ -1,0 +1,73 @@
+// Launch interfaces of the factorization and sweep kernels.
+#pragma once
+#include "common.cuh"
+
+namespace flam {
+
+struct CompressArgs {
+  Problem P;
+  const CompressTask* tasks;
+  int64_t* ipool;      // slf lists (reordered to [sk rd])
+  int64_t* cpool;      // neighbour candidates (filtered in place)
+  double* tpool;       // T slots
+  int32_t* permpool;   // local permutations
+  double* scratch;     // work matrices of boxes with n > kSmemN
+  CompressOut* out;
+  double rel_tol;      // rem(rank_or_tol, 1)
+  int kmax;            // floor(rank_or_tol)
+  int symm_n;          // 1: compress [A(nbr,slf); A(slf,nbr)'; Kpxy] (symm 'n')
+  double Tmax;
+  int64_t rrqr_iter;   // < 0: unlimited
+};
+
+size_t compress_smem_bytes(int n);
+int64_t compress_scratch_doubles(int n);
+void launch_compress(const CompressArgs& a, int ntask, size_t smem, cudaStream_t s);
+
+struct ElimArgs {
+  Problem P;
+  const ElimTask* tasks;
+  const ChildBlock* children;
+  const int64_t* ipool;
+  const double* tpool;
+  const int32_t* permpool;
+  const double* m_in;   // children's M blocks
+  double* m_out;        // this step's M blocks
+  double* fpool;        // factors
+  int32_t* ppool;       // LU permutations
+  double* scratch;      // work matrices of boxes with n > kSmemN
+  int32_t* status;      // OR of StatusBits
+  int symm;             // 'n', 's', 'p', 'h'
+};
+
+size_t elim_smem_bytes(int n);
+int64_t elim_scratch_doubles(int n);
+void launch_eliminate(const ElimArgs& a, int ntask, size_t smem, cudaStream_t s);
+
+// Segmented copies of int64 ids: dst[dst_off + i] = src[src_off + i], i < len.
+struct CopySeg {
+  int64_t src_off, dst_off, len;
+};
+void launch_gather_ids(const int64_t* src, int64_t* dst, const CopySeg* segs, int nseg, cudaStream_t s);
+
+// Sweeps over the factors of one step (rskelf_sv_*.m / rskelf_mv_*.m).
+// op: 0 sv upward, 1 sv downward, 2 mv upward, 3 mv downward; trans 0 = 'n', 1 = 'c'/'t'.
+struct SweepArgs {
+  const FacDesc* fac;
+  const int64_t* ipool;
+  const double* fpool;
+  const int32_t* ppool;
+  double* X;            // point-major: X[pt * ldx + c]
+  int64_t ldx;
+  int nrhs;
+  int op;
+  int trans;
+  int symm;
+};
+void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t s);
+
+// Layout changes for the user's column-major X (N x nrhs, ld) <-> point-major work array.
+void launch_to_pointmajor(const double* X, int64_t ld, int64_t N, int nrhs, double* W, cudaStream_t s);
+void launch_from_pointmajor(const double* W, int64_t N, int nrhs, double* X, int64_t ld, cudaStream_t s);
+
+}  // namespace flam

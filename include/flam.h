@@ -1,0 +1,194 @@
+/*
+ * flam.h -- C ABI of the B200 (sm_100a) recursive skeletonization factorization.
+ *
+ * This is the drop-in boundary for the reference's MATLAB/Octave entry points
+ *
+ *   F = rskelf(A, x, occ, rank_or_tol, pxyfun, opts)   rskelf/rskelf.m:109
+ *   Y = rskelf_sv(F, X, trans)                          rskelf/rskelf_sv.m:13
+ *   Y = rskelf_mv(F, X, trans)                          rskelf/rskelf_mv.m:13
+ *   T = hypoct(x, occ, lvlmax, ext)                     core/hypoct.m:51
+ *   P = hypoct_perm(T)                                  core/hypoct_perm.m:11
+ *
+ * A MEX/oct gateway (or ctypes, cgo, JNI ...) binds these symbols.  The
+ * reference's function handles A(I,J) and pxyfun(x,slf,nbr,l,ctr) are
+ * replaced by registry descriptors (flam_kernel, flam_proxy): the matrix is
+ * evaluated on the device, there is no callback into the host and no CPU
+ * fallback.
+ *
+ * Conventions
+ *   - Arrays are column-major like MATLAB: x is d x N (point-major), X is
+ *     N x nrhs with leading dimension ldx.
+ *   - Pointers may be host or device memory; the library detects which.
+ *   - Index arrays returned by the export calls are 0-based; a MATLAB
+ *     gateway adds 1.
+ *   - Every call returns a flam_status; flam_last_error() gives the message,
+ *     prefixed with the reference's error identifier ("FLAM:id:...").
+ *   - A handle is bound to the device that was current when it was created
+ *     and to the stream given in flam_opts (0: the legacy default stream).
+ *     Calls on one handle must not run concurrently from several threads.
+ */
+#ifndef FLAM_B200_H
+#define FLAM_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FLAM_API __attribute__((visibility("default")))
+#else
+#define FLAM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FLAM_OK = 0,
+  FLAM_ERR_ARG = 1,          /* invalid argument (FLAM:chksymm, FLAM:hypoct, FLAM:id ...) */
+  FLAM_ERR_NOT_SPD = 2,      /* chol of a redundant block failed (symm = 'p') */
+  FLAM_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  FLAM_ERR_NOMEM = 4,        /* device allocation failed */
+  FLAM_ERR_UNSUPPORTED = 5,  /* option not available on the device path */
+  FLAM_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
+  FLAM_ERR_ID_CHECK = 7,     /* posterior ID residual check failed */
+  FLAM_WARN_RRQR_MAXITER = 100, /* FLAM:id:maxIterCount (factor is still valid) */
+  FLAM_WARN_SINGULAR = 101      /* an LU pivot of a redundant block was exactly zero */
+} flam_status;
+
+/* Kernel registry: the matrix entry is A(i,j) = scale * w_j * K(x_i, x_j) for
+ * i != j and A(i,i) = dval.  Kernels follow the reference's test drivers. */
+typedef enum {
+  FLAM_KERNEL_LAPLACE2D = 0,     /* -log(r)/(2 pi)             rskelf/test/ie_circle.m:85-95   */
+  FLAM_KERNEL_LAPLACE2D_DL = 1,  /* (r . n_j)/(2 pi r^2)       rskelf/test/ie_circle.m:91-94   */
+  FLAM_KERNEL_LAPLACE3D = 2,     /* 1/(4 pi r)                 rskelf/test/ie_cube1.m:115-121  */
+  FLAM_KERNEL_GAUSSIAN = 3,      /* exp(-(param r)^2/2)        rskelf/test/cov_circle1.m:130   */
+  FLAM_KERNEL_MATERN32 = 4       /* (1+sqrt3 param r)e^{-sqrt3 param r} rskelf/test/cov_circle2.m:129 */
+} flam_kernel_kind;
+
+typedef struct {
+  int kind;               /* flam_kernel_kind */
+  double scale;           /* multiplies every off-diagonal entry */
+  double dval;            /* diagonal value A(i,i) */
+  double param;           /* inverse length scale for GAUSSIAN / MATERN32 */
+  const double* weights;  /* N column weights, or NULL (all ones) */
+  const double* normals;  /* d x N source normals (LAPLACE2D_DL), or NULL */
+} flam_kernel;
+
+/* Proxy registry (replaces pxyfun): far field of a box of size l, centre c. */
+typedef enum {
+  FLAM_PROXY_NONE = 0,    /* no pxyfun: naive global compression (rskelf.m:204) */
+  FLAM_PROXY_RING = 1,    /* p points 1.5(cos t, sin t).*l + c, ellipse filter   ie_circle.m:35,106-115 */
+  FLAM_PROXY_SPHERE = 2,  /* p Fibonacci points radius 1.5 .*l + c, ellipsoid filter  ie_cube1.m:131-140 */
+  FLAM_PROXY_ANNULUS = 3  /* base*t + 1.5 base.*l + c, t in [0, 3/param], box filter  cov_circle1.m:34-40,146-152 */
+} flam_proxy_kind;
+
+typedef struct {
+  int kind;          /* flam_proxy_kind */
+  int p;             /* number of reference points (directions for ANNULUS) */
+  int p_rad;         /* ANNULUS: radii per direction */
+  int kernel_kind;   /* kernel evaluated between proxy and box points */
+  double scale;      /* multiplies the proxy block */
+  double param;      /* kernel parameter for the proxy kernel */
+  int two_sided;     /* 1: rows [K diag(w_slf); wbar K] for weighted unsymmetric matrices */
+} flam_proxy;
+
+typedef struct {
+  int lvlmax;            /* maximum tree depth; <= 0 means Inf           (rskelf.m:114) */
+  const double* ext;     /* d x 2 root extent or NULL                     (rskelf.m:115) */
+  double Tmax;           /* ID entry bound, >= 1; INFINITY disables RRQR  (rskelf.m:116) */
+  int64_t rrqr_iter;     /* max RRQR iterations; < 0 means Inf            (rskelf.m:117) */
+  char symm;             /* 'n', 's', 'h' or 'p'                          (rskelf.m:118) */
+  int stop;              /* stop after this many levels; < 0 means Inf    (rskelf.m:119) */
+  int verb;              /* 1: print the per-level table                  (rskelf.m:120) */
+  void* stream;          /* cudaStream_t the handle runs on (NULL: default stream) */
+} flam_opts;
+
+typedef struct flam_factor flam_factor;
+
+/* Fill opts with the reference defaults (rskelf.m:112-120). */
+FLAM_API void flam_opts_default(flam_opts* opts);
+
+/* F = rskelf(A, x, occ, rank_or_tol, pxyfun, opts)   rskelf/rskelf.m:109-309 */
+FLAM_API flam_status flam_rskelf(const double* x, int d, int64_t N, const flam_kernel* A, double occ,
+                        double rank_or_tol, const flam_proxy* pxy, const flam_opts* opts,
+                        flam_factor** F);
+
+/* T = hypoct(x, occ, lvlmax, ext) alone: a handle holding only the tree
+ * (read it with flam_tree_export / flam_tree_perm).  lvlmax <= 0 means Inf,
+ * ext is d x 2 or NULL.   core/hypoct.m:51-171 */
+FLAM_API flam_status flam_hypoct(const double* x, int d, int64_t N, double occ, int lvlmax, const double* ext,
+                                 void* stream, flam_factor** T);
+
+/* Many independent problems in one pipeline: instance i has N[i] points at
+ * x + d * (N[0] + ... + N[i-1]) and matrix A[i].  Every step of the
+ * factorization runs all instances' boxes of the matching level in one launch.
+ * Semantically identical to ninst calls of flam_rskelf. */
+FLAM_API flam_status flam_rskelf_batched(int ninst, const double* x, int d, const int64_t* N,
+                                const flam_kernel* A, double occ, double rank_or_tol,
+                                const flam_proxy* pxy, const flam_opts* opts, flam_factor** F);
+
+/* Y = rskelf_sv(F, X, trans), in place on X (N x nrhs, leading dim ldx).
+ * rskelf/rskelf_sv.m:13-36.  For a batched handle N is the total over instances. */
+FLAM_API flam_status flam_rskelf_sv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans);
+
+/* Y = rskelf_mv(F, X, trans), in place.  rskelf/rskelf_mv.m:13-36. */
+FLAM_API flam_status flam_rskelf_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans);
+
+/* Sizes of a handle. */
+typedef struct {
+  int64_t N;          /* total points */
+  int ninst;          /* instances */
+  int d;
+  char symm;
+  int64_t nbox;       /* tree boxes (all instances) */
+  int nlvl_max;       /* deepest tree */
+  int64_t nfactor;    /* stored box factors */
+  int nstep;          /* factorization steps (levels processed, deepest instance) */
+  int64_t bytes;      /* device bytes held by the factor (pools) */
+  int64_t nrem;       /* points left uneliminated (partial factorization) */
+  double t_tree, t_factor;  /* seconds on the device (CUDA events) */
+} flam_info;
+
+FLAM_API flam_status flam_factor_info(const flam_factor* F, flam_info* info);
+
+/* Tree of instance `inst`, the reference's T = hypoct(...) struct flattened:
+ * nlvl, lvp (nlvl+1), l (d x nlvl), and per box ctr (d), prnt, children,
+ * neighbours and points as CSR arrays.  Call once with all array pointers NULL
+ * to get the sizes in *nbox, *nchld_tot, *nnbor_tot, *npts_tot, then again
+ * with host arrays of those sizes.   core/hypoct.m:15-37 */
+FLAM_API flam_status flam_tree_export(const flam_factor* F, int inst, int* nlvl, int64_t* nbox,
+                             int64_t* nchld_tot, int64_t* nnbor_tot, int64_t* npts_tot,
+                             int64_t* lvp, double* l, double* ctr, int64_t* prnt,
+                             int64_t* chld_ptr, int64_t* chld, int64_t* nbor_ptr, int64_t* nbor,
+                             int64_t* xi_ptr, int64_t* xi);
+
+/* P = hypoct_perm(T) for instance `inst` (N[inst] entries, 0-based). core/hypoct_perm.m:11-39 */
+FLAM_API flam_status flam_tree_perm(const flam_factor* F, int inst, int64_t* P);
+
+/* Factor list of instance `inst`: F.lvp (nstep+1 entries) and, per factor,
+ * k = |sk|, r = |rd|.  Arrays may be NULL to query *nfac / *nlvp. */
+FLAM_API flam_status flam_factor_sizes(const flam_factor* F, int inst, int64_t* nfac, int* nlvp,
+                              int64_t* lvp, int64_t* k, int64_t* r);
+
+/* Factor j of instance `inst` (rskelf.m:249-257): sk (k), rd (r), T (k x r),
+ * L (r x r), U (r x r), p (r), E (k x r), G (r x k).  Any pointer may be NULL.
+ * symm 'p': U, p, G untouched.  symm 'h': U holds the block-diagonal D, p and G untouched. */
+FLAM_API flam_status flam_factor_export(const flam_factor* F, int inst, int64_t j, int64_t* sk, int64_t* rd,
+                               double* T, double* L, double* U, int64_t* p, double* E, double* G);
+
+/* Per-level table of opts.verb (rskelf.m:267-272) for instance `inst`:
+ * rows of (lvl, nblk, nrem1, nrem2); returns the row count in *nrows. */
+FLAM_API flam_status flam_level_stats(const flam_factor* F, int inst, int* nrows, int64_t* rows);
+
+FLAM_API void flam_factor_free(flam_factor* F);
+
+/* Message of the last failed call on this thread ("FLAM:<fn>:<id>: text"). */
+FLAM_API const char* flam_last_error(void);
+
+/* Library version string. */
+FLAM_API const char* flam_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLAM_B200_H */
