@@ -5,9 +5,9 @@ Device code: ``flam_b200/csrc`` (sm_100a CUDA), exported through the C ABI of
 host-side mirror of the reference's MATLAB entry points.
 """
 from ._lib import FlamError, lib
-from .api import Factor, hypoct, hypoct_perm, rskelf, rskelf_batched, rskelf_mv, rskelf_sv
+from .api import Factor, hypoct, hypoct_perm, id, rskelf, rskelf_batched, rskelf_mv, rskelf_sv
 from .registry import Kernel, Proxy
 from . import problems
 
-__all__ = ["FlamError", "lib", "Factor", "hypoct", "hypoct_perm", "rskelf", "rskelf_batched", "rskelf_mv",
+__all__ = ["FlamError", "lib", "Factor", "hypoct", "hypoct_perm", "id", "rskelf", "rskelf_batched", "rskelf_mv",
            "rskelf_sv", "Kernel", "Proxy", "problems"]

@@ -19,9 +19,9 @@ STATUS = {
 
 # every symbol include/flam.h declares
 EXPORTS = (
-    "flam_opts_default", "flam_hypoct", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
+    "flam_opts_default", "flam_hypoct", "flam_id", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
     "flam_factor_info", "flam_tree_export", "flam_tree_perm", "flam_factor_sizes", "flam_factor_export",
-    "flam_level_stats", "flam_factor_free", "flam_last_error", "flam_version",
+    "flam_level_stats", "flam_factor_free", "flam_profile", "flam_last_error", "flam_version",
 )
 
 
@@ -37,13 +37,21 @@ class FlamProxy(C.Structure):
 
 class FlamOpts(C.Structure):
     _fields_ = [("lvlmax", C.c_int), ("ext", C.c_void_p), ("Tmax", C.c_double), ("rrqr_iter", C.c_int64),
-                ("symm", C.c_char), ("stop", C.c_int), ("verb", C.c_int), ("stream", C.c_void_p)]
+                ("symm", C.c_char), ("stop", C.c_int), ("verb", C.c_int), ("stream", C.c_void_p),
+                ("profile", C.c_int)]
 
 
 class FlamInfo(C.Structure):
     _fields_ = [("N", C.c_int64), ("ninst", C.c_int), ("d", C.c_int), ("symm", C.c_char), ("nbox", C.c_int64),
                 ("nlvl_max", C.c_int), ("nfactor", C.c_int64), ("nstep", C.c_int), ("bytes", C.c_int64),
                 ("nrem", C.c_int64), ("t_tree", C.c_double), ("t_factor", C.c_double)]
+
+
+class FlamProf(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("n_compress", C.c_int64), ("n_elim", C.c_int64), ("n_sweep", C.c_int64),
+                ("t_compress", C.c_double), ("t_elim", C.c_double), ("t_sweep", C.c_double),
+                ("flop_compress", C.c_double), ("flop_elim", C.c_double), ("flop_sweep", C.c_double),
+                ("byte_sweep", C.c_double)]
 
 
 class FlamError(RuntimeError):
@@ -76,6 +84,9 @@ def lib():
     L.flam_rskelf.restype = C.c_int
     L.flam_hypoct.argtypes = [P, C.c_int, C.c_int64, C.c_double, C.c_int, P, P, C.POINTER(P)]
     L.flam_hypoct.restype = C.c_int
+    L.flam_id.argtypes = [P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64, i64p, i64p, dp,
+                          i64p]
+    L.flam_id.restype = C.c_int
     L.flam_rskelf_batched.argtypes = [C.c_int, P, C.c_int, i64p, C.POINTER(FlamKernel), C.c_double, C.c_double,
                                       C.POINTER(FlamProxy), C.POINTER(FlamOpts), C.POINTER(P)]
     L.flam_rskelf_batched.restype = C.c_int
@@ -95,6 +106,8 @@ def lib():
     L.flam_factor_export.restype = C.c_int
     L.flam_level_stats.argtypes = [P, C.c_int, C.POINTER(C.c_int), i64p]
     L.flam_level_stats.restype = C.c_int
+    L.flam_profile.argtypes = [P, C.POINTER(FlamProf), C.c_int]
+    L.flam_profile.restype = C.c_int
     L.flam_factor_free.argtypes = [P]
     L.flam_factor_free.restype = None
     L.flam_last_error.argtypes = []

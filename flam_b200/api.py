@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib
 from .registry import Kernel, Proxy
 
-_OPT_KEYS = {"lvlmax", "ext", "Tmax", "rrqr_iter", "symm", "stop", "verb", "stream"}
+_OPT_KEYS = {"lvlmax", "ext", "Tmax", "rrqr_iter", "symm", "stop", "verb", "stream", "profile"}
 
 
 def _c_opts(opts):
@@ -49,6 +49,8 @@ def _c_opts(opts):
             o.verb = int(bool(v))
         elif k == "stream":
             o.stream = v
+        elif k == "profile":
+            o.profile = int(bool(v))
     return o, keep
 
 
@@ -63,12 +65,20 @@ class Factor:
         self._h = handle
         self.ninst = ninst
         self._keep = keep
+        self._free = _lib.lib().flam_factor_free
 
-    def __del__(self):
+    def free(self):
+        """Release the device memory now (the reference's ``clear F``)."""
         h = getattr(self, "_h", None)
         if h:
-            _lib.lib().flam_factor_free(h)
+            self._free(h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
     @property
     def handle(self):
@@ -163,6 +173,12 @@ class Factor:
             out.append(f)
         return dict(N=self._inst_sizes()[inst], lvp=lvp, factors=out, symm=symm)
 
+    def profile(self, reset=False):
+        """Launch accounting (kernel times, algorithmic flops/bytes, launch counts)."""
+        p = _lib.FlamProf()
+        _lib.check(_lib.lib().flam_profile(self._h, C.byref(p), int(bool(reset))))
+        return {f: getattr(p, f) for f, _ in p._fields_}
+
     def level_stats(self, inst=0):
         """Rows (lvl, nblk, start npts, end npts) of the opts.verb table (rskelf.m:267-272)."""
         n = C.c_int()
@@ -208,17 +224,28 @@ def _check_handles(A, pxyfun):
         raise _lib.FlamError(5, "FLAM:gpu:unsupportedHandle: pxyfun must be a registry Proxy, not a function handle")
 
 
+def _points(x):
+    """(pointer, d, N, keepalive) of d x N points: NumPy (host) or a CUDA tensor (device)."""
+    if _is_cuda_tensor(x):
+        import torch
+        if x.dtype != torch.float64 or x.dim() != 2 or x.stride(0) != 1 or x.stride(1) != x.shape[0]:
+            raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: x must be a float64 d x N column-major tensor "
+                                    "(e.g. pts.t() of a contiguous N x d tensor)")
+        return x.data_ptr(), x.shape[0], x.shape[1], x
+    a = np.asfortranarray(x, dtype=np.float64)
+    return a.ctypes.data, a.shape[0], a.shape[1], a
+
+
 def rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None):
     """F = rskelf(A, x, occ, rank_or_tol, pxyfun, opts)   rskelf/rskelf.m:109-309."""
     _check_handles(A, pxyfun)
-    x = np.asfortranarray(x, dtype=np.float64)
-    d, N = x.shape
+    ptr, d, N, keep_x = _points(x)
     o, keep = _c_opts(opts)
     ka = A.c_struct()
     px = (pxyfun or Proxy("none", 1)).c_struct()
     h = C.c_void_p()
-    _lib.check(_lib.lib().flam_rskelf(x.ctypes.data, d, N, C.byref(ka), float(occ), float(rank_or_tol), C.byref(px),
-                                      C.byref(o), C.byref(h)))
+    _lib.check(_lib.lib().flam_rskelf(C.c_void_p(ptr), d, N, C.byref(ka), float(occ), float(rank_or_tol),
+                                      C.byref(px), C.byref(o), C.byref(h)))
     return Factor(h.value, 1)
 
 
@@ -241,20 +268,26 @@ def rskelf_batched(As, xs, occ, rank_or_tol, pxyfun=None, opts=None):
     return F
 
 
+def _fresh_copy(X):
+    """A new column-major copy of X (MATLAB value semantics: the input is never modified)."""
+    if _is_cuda_tensor(X):
+        import torch
+        if X.dim() == 1:
+            return X.clone()
+        Y = torch.empty_strided(tuple(X.shape), (1, X.shape[0]), dtype=torch.float64, device=X.device)
+        Y.copy_(X)
+        return Y
+    return np.array(X, dtype=np.float64, order="F", copy=True)
+
+
 def rskelf_sv(F, X, trans="n"):
     """Y = rskelf_sv(F, X, trans): returns a new array (MATLAB value semantics)."""
-    if _is_cuda_tensor(X):
-        Y = X.clone() if X.dim() == 1 else X.t().contiguous().t()
-        return F.sv_(Y, trans)
-    return F.sv_(np.array(X, dtype=np.float64, order="F", copy=True), trans)
+    return F.sv_(_fresh_copy(X), trans)
 
 
 def rskelf_mv(F, X, trans="n"):
     """Y = rskelf_mv(F, X, trans): returns a new array."""
-    if _is_cuda_tensor(X):
-        Y = X.clone() if X.dim() == 1 else X.t().contiguous().t()
-        return F.mv_(Y, trans)
-    return F.mv_(np.array(X, dtype=np.float64, order="F", copy=True), trans)
+    return F.mv_(_fresh_copy(X), trans)
 
 
 def hypoct(x, occ, lvlmax=math.inf, ext=None):
@@ -271,6 +304,23 @@ def hypoct(x, occ, lvlmax=math.inf, ext=None):
     F = Factor(h.value, 1)
     F._sizes = [N]
     return F
+
+
+def id(A, rank_or_tol, Tmax=2.0, rrqr_iter=math.inf):  # noqa: A001 - the reference's name
+    """[sk, rd, T, niter] = id(A, rank_or_tol, Tmax, rrqr_iter) on the device.   core/id.m:44-248."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    m, n = A.shape
+    k = C.c_int64()
+    it = C.c_int64()
+    perm = np.zeros(max(n, 1), np.int64)
+    T = np.zeros(max(n * n // 4 + 1, 1))
+    _lib.check(_lib.lib().flam_id(A.ctypes.data if A.size else None, m, n, max(m, 1), float(rank_or_tol), float(Tmax),
+                                  -1 if rrqr_iter in (None, math.inf) else int(rrqr_iter), C.byref(k),
+                                  perm.ctypes.data_as(C.POINTER(C.c_int64)), T.ctypes.data_as(C.POINTER(C.c_double)),
+                                  C.byref(it)))
+    kk = k.value
+    Tm = T[:kk * (n - kk)].reshape(n - kk, kk).T.copy() if 0 < kk < n else np.zeros((kk, n - kk))
+    return perm[:kk].copy(), perm[kk:n].copy(), Tm, it.value
 
 
 def hypoct_perm(T):

@@ -10,6 +10,7 @@
 // Reference loop being replaced: rskelf/rskelf.m:168-263.  Steps run the
 // boxes of every instance whose level is (its depth - step), leaves first.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -114,6 +115,9 @@ struct HostFac {
 struct StepDev {
   DBuf<FacDesc> fac;
   int nfac = 0, kmax = 0, rmax = 0;
+  double flop_per_rhs = 0;   // sum over factors of 4kr + r^2 (one direction, one right-hand side)
+  double fac_bytes = 0;      // sum of 8 (2kr + r^2): factor data one direction reads
+  double x_rows = 0;         // sum of k + r
 };
 
 struct LevelStat {
@@ -159,6 +163,8 @@ struct flam_factor {
   std::vector<int64_t> rem;  // remaining points per instance
   double t_tree = 0, t_factor = 0;
   int64_t warn = 0;
+  bool profile = false;
+  mutable flam_prof prof{};
 
   ~flam_factor() {
     if (!s && !x.p) return;
@@ -238,6 +244,21 @@ void proxy_points(const flam_proxy& px, int d, std::vector<double>& pts, std::ve
   }
 }
 
+// Stream-ordered allocations come from the device's default pool; keep freed
+// memory in the pool instead of returning it to the driver at every
+// synchronisation, so the per-level work buffers are recycled, not remapped.
+// (Process-local runtime state; nothing about the GPU itself changes.)
+void keep_pool_memory(int dev) {
+  static bool done[64] = {};
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[dev] = true;
+}
+
 char chksymm(char c) {
   c = (char)std::tolower((unsigned char)c);
   if (c != 'n' && c != 's' && c != 'h' && c != 'p')
@@ -279,6 +300,7 @@ void build_tree(flam_factor& F, double occ, const flam_opts& o) {
     DBuf<double> part;
     part.resize((int64_t)ninst * nchunk * 2 * d, s);
     tree_extent(F.x.p, d, inst_off_d.p, ninst, nchunk, part.p, s);
+    F.prof.launches += 1;
     auto ph = download(part.p, part.n, s);
     for (int i = 0; i < ninst; ++i)
       for (int q = 0; q < d; ++q) {
@@ -405,6 +427,7 @@ void build_tree(flam_factor& F, double occ, const flam_opts& o) {
     const int64_t L = (int64_t)nl * (ntot + 1);
     flags.resize(L + 1, s);
     scr32.resize(scan_scratch_elems(std::max<int64_t>(L, b1 - b0)) + 1, s);
+    F.prof.launches += 9;  // flags, 2 scans of 3 kernels, count, children/scatter below
     tree_level_flags(t, ntot, b0, b1, iocc, 1, ldiv_d.p, flags.p, nl, s);
     exclusive_scan<int32_t>(flags.p, flags.p, L, scr32.p, s);
     nchtmp.resize(b1 - b0 + 1, s);
@@ -441,6 +464,7 @@ void build_tree(flam_factor& F, double occ, const flam_opts& o) {
       cnt.resize(nb + 1, s);
       scr64.resize(scan_scratch_elems(nb) + 1, s);
       TreeDev t = tdev();
+      F.prof.launches += 5;
       tree_neighbours(t, b0, b1, 0, cnt.p, s);
       exclusive_scan<int64_t>(cnt.p, cnt.p, nb, scr64.p, s);
       auto h = download(cnt.p, (int64_t)nb + 1, s);
@@ -465,6 +489,7 @@ void build_tree(flam_factor& F, double occ, const flam_opts& o) {
     for (int Dd = 1; Dd < maxdepth; ++Dd) tree_perm_offsets(t, (int32_t)lvb[Dd - 1], (int32_t)lvb[Dd], off.p, s);
     F.hperm.resize(ntot, s);
     tree_perm_fill(t, (int32_t)nbox, off.p, F.hperm.p, s);
+    F.prof.launches += maxdepth;
     off.release(s);
   }
   CK(cudaEventRecord(e1, s));
@@ -568,11 +593,12 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   P.npxy = F.npxy;
   int cur = 0;  // M pool written this step
   int64_t fpool_top = 0, ppool_top = 0;
-  const bool prof = std::getenv("FLAM_PROFILE") != nullptr;
-  cudaEvent_t pe[4];
+  const bool prof = F.profile;
+  const bool prof_print = std::getenv("FLAM_PROFILE") != nullptr;
+  cudaEvent_t pe[4] = {};
+
   if (prof)
     for (auto& e : pe) CK(cudaEventCreate(&e));
-
   for (int step = 0; step < maxsteps && step < stop; ++step) {
     // ---- boxes of this step: level nlvl_i - step of each instance
     std::vector<int32_t> boxes;
@@ -680,7 +706,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     launch_gather_ids(F.ipool.p, cpool.p, csegs.p, (int)cs.size(), s);
     ctask.upload(ct, s);
     cout.resize(nb, s);
-    CompressArgs ca;
+    CompressArgs ca{};
     ca.P = P;
     ca.tasks = ctask.p;
     ca.ipool = F.ipool.p;
@@ -694,6 +720,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ca.symm_n = F.symm == 'n' ? 1 : 0;
     ca.Tmax = o.Tmax;
     ca.rrqr_iter = o.rrqr_iter;
+    ca.Aexp = nullptr;
+    ca.lda = 0;
+    F.prof.launches += 2 + 1;  // two id gathers, compress
+    F.prof.n_compress += 1;
     if (prof) CK(cudaEventRecord(pe[0], s));
     launch_compress(ca, nb, compress_smem_bytes(nmax_small), s);
     CK(cudaGetLastError());
@@ -758,7 +788,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     mpool[cur].resize(std::max<int64_t>(mtop, 1), s);
     etask.upload(et, s);
     chb.upload(ch, s);
-    ElimArgs ea;
+    ElimArgs ea{};
     ea.P = P;
     ea.tasks = etask.p;
     ea.children = chb.p;
@@ -772,12 +802,32 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ea.scratch = scratch.p;
     ea.status = status.p;
     ea.symm = F.symm;
+    F.prof.launches += 1;
+    F.prof.n_elim += 1;
+    for (int q = 0; q < nb; ++q) {  // algorithmic work of this step (reference operations per box)
+      const double n = (double)nslf[q], m = (double)co[q].m, k = co[q].k, r = n - k;
+      if (m > 0 && n > 0) {
+        const double a = std::max(m, n), b = std::min(m, n);
+        F.prof.flop_compress += 2 * a * b * b - 2.0 / 3.0 * b * b * b + k * k * r;  // xGEQP3 + R11\R12
+      }
+      if (r > 0) {
+        const double fac = chol ? r * r * r / 3 + k * r * r : 2.0 / 3.0 * r * r * r + 2 * k * r * r;
+        F.prof.flop_elim += 4 * k * r * n + fac + 2 * k * k * r;
+      }
+    }
     if (prof) CK(cudaEventRecord(pe[2], s));
     launch_eliminate(ea, nb, elim_smem_bytes(nmax_e), s);
     CK(cudaGetLastError());
     if (prof) {
       CK(cudaEventRecord(pe[3], s));
       CK(cudaEventSynchronize(pe[3]));
+      float tc = 0, tel = 0;
+      CK(cudaEventElapsedTime(&tc, pe[0], pe[1]));
+      CK(cudaEventElapsedTime(&tel, pe[2], pe[3]));
+      F.prof.t_compress += tc * 1e-3;
+      F.prof.t_elim += tel * 1e-3;
+    }
+    if (prof && prof_print) {
       float tc = 0, tel = 0;
       CK(cudaEventElapsedTime(&tc, pe[0], pe[1]));
       CK(cudaEventElapsedTime(&tel, pe[2], pe[3]));
@@ -799,6 +849,12 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     sd.nfac = (int)fd.size();
     sd.kmax = kmx;
     sd.rmax = rmx;
+    for (const FacDesc& f : fd) {
+      const double k = f.k, r = f.r;
+      sd.flop_per_rhs += 4 * k * r + r * r;
+      sd.fac_bytes += 8 * (2 * k * r + r * r);
+      sd.x_rows += k + r;
+    }
     F.steps.push_back(std::move(sd));
     // ---- host state for the next step (rskelf.m:245-261)
     for (int q = 0; q < nb; ++q) {
@@ -830,6 +886,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   F.t_factor = ms * 1e-3;
   CK(cudaEventDestroy(e0));
   CK(cudaEventDestroy(e1));
+  if (prof)
+    for (auto& e : pe) CK(cudaEventDestroy(e));
   for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1]}) b->release(s);
   cpool.release(s);
   permpool.release(s);
@@ -903,7 +961,9 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
 
   std::unique_ptr<flam_factor> F(new flam_factor());
   CK(cudaGetDevice(&F->dev));
+  keep_pool_memory(F->dev);
   F->s = (cudaStream_t)o.stream;
+  F->profile = o.profile != 0 || std::getenv("FLAM_PROFILE") != nullptr;
   F->d = d;
   F->ninst = ninst;
   F->symm = symm;
@@ -964,8 +1024,20 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
   F->pxy_pts.upload(pts, s);
   if (!shift.empty()) F->pxy_shift.upload(shift, s);
 
+  const bool pp = std::getenv("FLAM_PROFILE") != nullptr;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto t0 = now();
+  CK(cudaStreamSynchronize(s));
+  auto t1 = now();
   build_tree(*F, occ, o);
+  auto t2 = now();
   factorize(*F, rank_or_tol, o);
+  auto t3 = now();
+  if (pp)
+    fprintf(stderr, "[flam] create: upload %.3f ms  tree %.3f ms (device %.3f)  factorize %.3f ms (device %.3f)\n",
+            std::chrono::duration<double, std::milli>(t1 - t0).count(),
+            std::chrono::duration<double, std::milli>(t2 - t1).count(), F->t_tree * 1e3,
+            std::chrono::duration<double, std::milli>(t3 - t2).count(), F->t_factor * 1e3);
   if (o.verb) print_table(*F);
   *out = F.release();
   if ((*out)->warn & 1) {
@@ -986,6 +1058,15 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   if (nrhs == 0 || F->Ntot == 0) return FLAM_OK;
   if (!X) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: X is NULL");
   cudaStream_t s = F->s;
+  const bool pp = std::getenv("FLAM_PROFILE") != nullptr;
+  cudaEvent_t pev[6] = {};
+  if (pp)
+    for (auto& e : pev) CK(cudaEventCreate(&e));
+  auto mark = [&](int i) {
+    if (pp) CK(cudaEventRecord(pev[i], s));
+  };
+  auto hstart = std::chrono::steady_clock::now();
+  mark(0);
   const int t = trans == 'n' ? 0 : 1;   // real data: 't' == 'c' (rskelf_sv.m:22)
   const int64_t N = F->Ntot;
   const bool dev = is_device_ptr(X);
@@ -1000,8 +1081,10 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
     ld = N;
   }
   W.resize(N * nrhs, s);
+  mark(1);
   launch_to_pointmajor(Xd, ld, N, (int)nrhs, W.p, s);
-  SweepArgs a;
+  mark(2);
+  SweepArgs a{};
   a.ipool = F->ipool.p;
   a.fpool = F->fpool.p;
   a.ppool = F->ppool.p;
@@ -1011,24 +1094,60 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   a.trans = t;
   a.symm = F->symm;
   const int ns = (int)F->steps.size();
-  a.op = solve ? 0 : 2;
-  for (int q = 0; q < ns; ++q) {
-    a.fac = F->steps[q].fac.p;
-    launch_sweep(a, F->steps[q].nfac, F->steps[q].kmax, F->steps[q].rmax, s);
+  cudaEvent_t ev[2] = {};
+  if (F->profile) {
+    CK(cudaEventCreate(&ev[0]));
+    CK(cudaEventCreate(&ev[1]));
   }
+  auto sweep = [&](int q) {
+    const StepDev& sd = F->steps[q];
+    a.fac = sd.fac.p;
+    if (sd.nfac == 0) return;
+    if (F->profile) CK(cudaEventRecord(ev[0], s));
+    launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
+    F->prof.launches += 1;
+    F->prof.n_sweep += 1;
+    F->prof.flop_sweep += sd.flop_per_rhs * (double)nrhs;
+    F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)nrhs;
+    if (F->profile) {
+      CK(cudaEventRecord(ev[1], s));
+      CK(cudaEventSynchronize(ev[1]));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      F->prof.t_sweep += ms * 1e-3;
+    }
+  };
+  F->prof.launches += 2;  // layout changes
+  a.op = solve ? 0 : 2;
+  for (int q = 0; q < ns; ++q) sweep(q);
   a.op = solve ? 1 : 3;
-  for (int q = ns - 1; q >= 0; --q) {
-    a.fac = F->steps[q].fac.p;
-    launch_sweep(a, F->steps[q].nfac, F->steps[q].kmax, F->steps[q].rmax, s);
+  for (int q = ns - 1; q >= 0; --q) sweep(q);
+  if (F->profile) {
+    CK(cudaEventDestroy(ev[0]));
+    CK(cudaEventDestroy(ev[1]));
   }
   CK(cudaGetLastError());
+  mark(3);
   launch_from_pointmajor(W.p, N, (int)nrhs, Xd, ld, s);
+  mark(4);
   if (!dev)
     CK(cudaMemcpy2DAsync(X, sizeof(double) * ldx, tmp.p, sizeof(double) * N, sizeof(double) * N, nrhs,
                          cudaMemcpyDeviceToHost, s));
   W.release(s);
   tmp.release(s);
+  mark(5);
   if (!dev) CK(cudaStreamSynchronize(s));
+  if (pp) {
+    auto henq = std::chrono::steady_clock::now();
+    CK(cudaEventSynchronize(pev[5]));
+    auto hend = std::chrono::steady_clock::now();
+    float a[5];
+    for (int i = 0; i < 5; ++i) CK(cudaEventElapsedTime(&a[i], pev[i], pev[i + 1]));
+    fprintf(stderr, "[flam] apply: alloc %.3f  to_pm %.3f  sweeps %.3f  from_pm %.3f  free %.3f ms  (host enqueue %.3f, wait %.3f ms)\n",
+            a[0], a[1], a[2], a[3], a[4], std::chrono::duration<double, std::milli>(henq - hstart).count(),
+            std::chrono::duration<double, std::milli>(hend - henq).count());
+    for (auto& e : pev) CK(cudaEventDestroy(e));
+  }
   return FLAM_OK;
 }
 
@@ -1060,6 +1179,7 @@ void flam_opts_default(flam_opts* o) {
   o->stop = -1;
   o->verb = 0;
   o->stream = nullptr;
+  o->profile = 0;
 }
 
 flam_status flam_rskelf(const double* x, int d, int64_t N, const flam_kernel* A, double occ, double rank_or_tol,
@@ -1093,6 +1213,101 @@ flam_status flam_hypoct(const double* x, int d, int64_t N, double occ, int lvlma
     F->inst_lvp.assign(1, {0});
     F->stats.assign(1, {});
     *T = F.release();
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_id(const double* A, int64_t m, int64_t n, int64_t lda, double rank_or_tol, double Tmax,
+                    int64_t rrqr_iter, int64_t* k, int64_t* perm, double* T, int64_t* niter) {
+  return guard([&] {
+    if (!(rank_or_tol >= 0)) fail(FLAM_ERR_ARG, "FLAM:id:invalidRankOrTol: Rank or tolerance must be nonnegative.");
+    if (!(Tmax >= 1)) fail(FLAM_ERR_ARG, "FLAM:id:invalidTmax: Interpolation matrix entry bound must be >= 1.");
+    if (m < 0 || n < 0 || (m > 0 && lda < m)) fail(FLAM_ERR_ARG, "FLAM:id:invalidArg: bad matrix dimensions");
+    if (n > 4096 || m > (int64_t)1 << 30) fail(FLAM_ERR_ARG, "FLAM:id:invalidArg: matrix too large for flam_id");
+    if (!k || !perm) fail(FLAM_ERR_ARG, "FLAM:id:invalidArg: NULL output");
+    cudaStream_t s = nullptr;
+    if (n == 0) {
+      *k = 0;
+      if (niter) *niter = 0;
+      return FLAM_OK;
+    }
+    DBuf<double> Ad, tp, scr, dummy;
+    DBuf<int64_t> ids, cp;
+    DBuf<int32_t> pp;
+    DBuf<CompressTask> tk;
+    DBuf<CompressOut> co;
+    DBuf<InstParams> ipd;
+    Ad.resize(std::max<int64_t>(m * n, 1), s);
+    if (m > 0) CK(cudaMemcpy2DAsync(Ad.p, sizeof(double) * m, A, sizeof(double) * lda, sizeof(double) * m, n,
+                                    cudaMemcpyDefault, s));
+    std::vector<int64_t> iv(n);
+    for (int64_t q = 0; q < n; ++q) iv[q] = q;
+    ids.upload(iv, s);
+    cp.resize(1, s);
+    tp.resize(n * n / 4 + 1, s);
+    pp.resize(n, s);
+    CompressTask t{};
+    t.slf_off = 0;
+    t.cand_off = 0;
+    t.T_off = 0;
+    t.perm_off = 0;
+    t.n = (int32_t)n;
+    t.ncand = (int32_t)m;
+    t.flags = 0;
+    if (n > kSmemN) {
+      scr.resize(compress_scratch_doubles((int)n), s);
+      t.scr_off = 0;
+    } else {
+      scr.resize(1, s);
+      t.scr_off = -1;
+    }
+    tk.upload(std::vector<CompressTask>{t}, s);
+    co.resize(1, s);
+    InstParams ip{};
+    ipd.upload(std::vector<InstParams>{ip}, s);
+    dummy.resize(4, s);
+    CompressArgs ca{};
+    ca.P.d = 1;
+    ca.P.x = dummy.p;
+    ca.P.ip = ipd.p;
+    ca.P.pxy_pts = dummy.p;
+    ca.tasks = tk.p;
+    ca.ipool = ids.p;
+    ca.cpool = cp.p;
+    ca.tpool = tp.p;
+    ca.permpool = pp.p;
+    ca.scratch = scr.p;
+    ca.out = co.p;
+    ca.rel_tol = std::fmod(rank_or_tol, 1.0);
+    ca.kmax = (int)std::min<double>(std::floor(rank_or_tol), 2e9);
+    ca.symm_n = 0;
+    ca.Tmax = Tmax;
+    ca.rrqr_iter = rrqr_iter;
+    ca.Aexp = Ad.p;
+    ca.lda = m;
+    launch_compress(ca, 1, compress_smem_bytes((int)n), s);
+    CK(cudaGetLastError());
+    auto o = download(co.p, 1, s);
+    auto pv = download(pp.p, n, s);
+    *k = o[0].k;
+    for (int64_t q = 0; q < n; ++q) perm[q] = pv[q];
+    if (niter) *niter = o[0].niter;
+    if (T && o[0].k > 0 && o[0].k < n) {
+      auto tv = download(tp.p, (int64_t)o[0].k * (n - o[0].k), s);
+      std::copy(tv.begin(), tv.end(), T);
+    }
+    for (auto* b : {&Ad, &tp, &scr, &dummy}) b->release(s);
+    ids.release(s);
+    cp.release(s);
+    pp.release(s);
+    tk.release(s);
+    co.release(s);
+    ipd.release(s);
+    CK(cudaStreamSynchronize(s));
+    if (o[0].status & ST_RRQR_CAP) {
+      g_err = "FLAM:id:maxIterCount: Maximum number of RRQR iterations reached.";
+      return FLAM_WARN_RRQR_MAXITER;
+    }
     return FLAM_OK;
   });
 }
@@ -1295,6 +1510,15 @@ flam_status flam_level_stats(const flam_factor* F, int inst, int* nrows, int64_t
 }
 
 void flam_factor_free(flam_factor* F) { delete F; }
+
+flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset) {
+  return guard([&] {
+    if (!F) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: NULL factor");
+    if (out) *out = F->prof;
+    if (reset) F->prof = flam_prof{};
+    return FLAM_OK;
+  });
+}
 
 const char* flam_last_error(void) { return g_err.c_str(); }
 

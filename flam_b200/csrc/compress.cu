@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "rrqr.cuh"
 
 namespace flam {
 namespace {
@@ -91,271 +92,6 @@ __device__ __forceinline__ double row_entry(const Problem& P, const InstParams& 
     default:
       return 0.0;
   }
-}
-
-// Givens rotation zeroing b in (a; b): returns c, s with [c s; -s c] (a; b) = (r; 0).
-__device__ __forceinline__ void rot(double a, double b, double& c, double& s) {
-  if (b == 0.0) {
-    c = 1.0;
-    s = 0.0;
-    return;
-  }
-  const double r = hypot(a, b);
-  c = a / r;
-  s = b / r;
-}
-
-__device__ void apply_rows(double* R, int ld, int r0, int c0, int c1, double c, double s) {
-  for (int col = c0; col < c1; ++col) {
-    const double a = R[r0 + (int64_t)col * ld], b = R[r0 + 1 + (int64_t)col * ld];
-    R[r0 + (int64_t)col * ld] = c * a + s * b;
-    R[r0 + 1 + (int64_t)col * ld] = -s * a + c * b;
-  }
-}
-
-// Swap columns i and k-1 of R11 (k x k) and re-triangularise (id.m:134,217).
-__device__ void swap_retri(double* R, int ld, int i, int k) {
-  for (int row = 0; row < k; ++row) {
-    double t = R[row + (int64_t)i * ld];
-    R[row + (int64_t)i * ld] = R[row + (int64_t)(k - 1) * ld];
-    R[row + (int64_t)(k - 1) * ld] = t;
-  }
-  double c, s;
-  for (int row = k - 1; row > i; --row) {  // clear the spike in column i bottom-up
-    rot(R[row - 1 + (int64_t)i * ld], R[row + (int64_t)i * ld], c, s);
-    apply_rows(R, ld, row - 1, i, k, c, s);
-    R[row + (int64_t)i * ld] = 0.0;
-  }
-  for (int col = i + 1; col < k - 1; ++col) {  // clear the subdiagonal left behind
-    rot(R[col + (int64_t)col * ld], R[col + 1 + (int64_t)col * ld], c, s);
-    apply_rows(R, ld, col, col, k, c, s);
-    R[col + 1 + (int64_t)col * ld] = 0.0;
-  }
-}
-
-// x = R[0:k,0:k] \ b (upper triangular), sequential.
-__device__ void trisolve(const double* R, int ld, int k, const double* b, double* x) {
-  for (int i = k - 1; i >= 0; --i) {
-    double v = b[i];
-    for (int j = i + 1; j < k; ++j) v -= R[i + (int64_t)j * ld] * x[j];
-    x[i] = v / R[i + (int64_t)i * ld];
-  }
-}
-
-// Sequential RRQR refinement of id.m:117-236 on thread 0.  R holds `rows` rows
-// (R11 | T) over n columns; returns the final rank, updates jpvt, niter.
-__device__ int rrqr_serial(double* R, int ld, int n, int k, int rows, int* jpvt, double tol, double Tmax,
-                           int64_t rrqr_iter, double* aux, int* niter_out, int* capped) {
-  double* r2 = aux;            // k
-  double* c2 = aux + n;        // n - k (+1)
-  double* u = aux + 2 * n;     // k
-  double* tv = aux + 3 * n;    // scratch
-  const double f2 = Tmax * Tmax;
-  int niter = 0;
-  // c2 = column norms^2 of R22, r2 = row norms^2 of inv(R11)
-  for (int j = 0; j < n - k; ++j) {
-    double s = 0.0;
-    for (int row = k; row < rows; ++row) s += R[row + (int64_t)(k + j) * ld] * R[row + (int64_t)(k + j) * ld];
-    c2[j] = s;
-  }
-  for (int i = 0; i < k; ++i) r2[i] = 0.0;
-  for (int j = 0; j < k; ++j) {
-    for (int i = 0; i < k; ++i) u[i] = (i == j) ? 1.0 : 0.0;
-    trisolve(R, ld, k, u, tv);
-    for (int i = 0; i < k; ++i) r2[i] += tv[i] * tv[i];
-  }
-  bool conv = false;
-  while ((rrqr_iter < 0 || niter < rrqr_iter) && niter < kRrqrCap) {
-    double t2 = -1.0;
-    int bi = 0, bj = 0;
-    for (int j = 0; j < n - k; ++j)
-      for (int i = 0; i < k; ++i) {
-        const double tij = R[i + (int64_t)(k + j) * ld];
-        const double v = fabs(tij * tij + r2[i] * c2[j]);
-        if (v > t2) {
-          t2 = v;
-          bi = i;
-          bj = j;
-        }
-      }
-    if (t2 <= f2) {
-      conv = true;
-      break;
-    }
-    ++niter;
-    if (bi < k - 1) {  // swap i-th and k-th columns (id.m:132-138)
-      int t = jpvt[bi];
-      jpvt[bi] = jpvt[k - 1];
-      jpvt[k - 1] = t;
-      swap_retri(R, ld, bi, k);
-      for (int col = k; col < n; ++col) {
-        double a = R[bi + (int64_t)col * ld];
-        R[bi + (int64_t)col * ld] = R[k - 1 + (int64_t)col * ld];
-        R[k - 1 + (int64_t)col * ld] = a;
-      }
-      double a = r2[bi];
-      r2[bi] = r2[k - 1];
-      r2[k - 1] = a;
-    }
-    if (bj > 0) {  // swap (k+1)-th and (k+j)-th columns (id.m:141-145)
-      int t = jpvt[k];
-      jpvt[k] = jpvt[k + bj];
-      jpvt[k + bj] = t;
-      for (int row = 0; row < rows; ++row) {
-        double a = R[row + (int64_t)k * ld];
-        R[row + (int64_t)k * ld] = R[row + (int64_t)(k + bj) * ld];
-        R[row + (int64_t)(k + bj) * ld] = a;
-      }
-      double a = c2[0];
-      c2[0] = c2[bj];
-      c2[bj] = a;
-    }
-    // downdate inverse row norms (id.m:148-149)
-    if (k > 1) {
-      trisolve(R, ld, k - 1, R + (int64_t)(k - 1) * ld, tv);
-      const double rkk = R[k - 1 + (int64_t)(k - 1) * ld];
-      for (int i = 0; i < k - 1; ++i) r2[i] -= fabs(tv[i] / rkk) * fabs(tv[i] / rkk);
-    }
-    r2[k - 1] = 0.0;
-    if (rows == k) {  // id.m:164-167
-      for (int i = 0; i < k; ++i) u[i] = R[i + (int64_t)k * ld];
-      for (int i = 0; i < k; ++i) {
-        double s = 0.0;
-        for (int j = i; j < k; ++j) s += R[i + (int64_t)j * ld] * u[j];
-        tv[i] = s;
-      }
-      for (int i = 0; i < k; ++i) R[i + (int64_t)k * ld] = tv[i];
-      for (int i = 0; i < k - 1; ++i) R[i + (int64_t)(k - 1) * ld] = 0.0;
-      R[k - 1 + (int64_t)(k - 1) * ld] = 1.0;
-    } else {  // id.m:168-198 (fixed-rank truncation leaves an R22 block)
-      const int h = rows - k;   // length of the Householder vector
-      double* v = tv;           // rows k..rows-1
-      double nv = 0.0;
-      for (int q = 0; q < h; ++q) v[q] = R[k + q + (int64_t)k * ld];
-      const double rkk1 = R[k + (int64_t)k * ld];
-      v[0] += sqrt(c2[0]) * (rkk1 < 0.0 ? -1.0 : 1.0);
-      for (int q = 0; q < h; ++q) nv += v[q] * v[q];
-      nv = sqrt(nv);
-      for (int q = 0; q < h; ++q) v[q] /= nv;
-      for (int col = k + 1; col < n; ++col) {
-        double s = 0.0;
-        for (int q = 0; q < h; ++q) s += v[q] * R[k + q + (int64_t)col * ld];
-        for (int q = 0; q < h; ++q) R[k + q + (int64_t)col * ld] -= 2.0 * v[q] * s;
-      }
-      for (int q = 1; q < h; ++q) R[k + q + (int64_t)k * ld] = 0.0;
-      R[k + (int64_t)k * ld] = sqrt(c2[0]);
-      // restore entries of T to "R space"
-      for (int i = 0; i < k; ++i) {
-        double s = 0.0;
-        for (int j = i; j < k; ++j) s += R[i + (int64_t)j * ld] * R[j + (int64_t)k * ld];
-        u[i] = s;
-      }
-      for (int i = 0; i < k; ++i) R[i + (int64_t)k * ld] = u[i];
-      const double rkk = R[k - 1 + (int64_t)(k - 1) * ld];
-      for (int col = k + 1; col < n; ++col) R[k - 1 + (int64_t)col * ld] *= rkk;
-      // r = R(1:k,k) and s = R(k,k+2:end) are kept in aux tail
-      double* rv = aux + 4 * n;       // k
-      double* sv = aux + 5 * n;       // n - k - 1
-      for (int i = 0; i < k; ++i) rv[i] = R[i + (int64_t)(k - 1) * ld];
-      for (int col = k + 1; col < n; ++col) sv[col - k - 1] = R[k - 1 + (int64_t)col * ld];
-      for (int col = k; col < n; ++col) c2[col - k] -= R[k + (int64_t)col * ld] * R[k + (int64_t)col * ld];
-      {  // MATLAB givens(R(k,k+1), R(k+1,k+1)) applied to rows k, k+1 over columns k..end
-        const double a = R[k - 1 + (int64_t)k * ld], b = R[k + (int64_t)k * ld];
-        double c, s;
-        if (a == 0.0) {
-          c = 0.0;
-          s = 1.0;
-        } else {
-          const double nr = hypot(a, b);
-          c = fabs(a) / nr;
-          s = (a < 0.0 ? -1.0 : 1.0) * (b / nr);
-        }
-        apply_rows(R, ld, k - 1, k - 1, n, c, s);
-      }
-      for (int col = k; col < n; ++col) c2[col - k] += R[k + (int64_t)col * ld] * R[k + (int64_t)col * ld];
-      c2[0] = R[k + (int64_t)(k - 1) * ld] * R[k + (int64_t)(k - 1) * ld];
-      const double tmp = R[k - 1 + (int64_t)(k - 1) * ld];
-      R[k - 1 + (int64_t)(k - 1) * ld] = rv[k - 1];
-      trisolve(R, ld, k, R + (int64_t)k * ld, u);
-      R[k - 1 + (int64_t)(k - 1) * ld] = tmp;
-      trisolve(R, ld, k - 1, rv, tv);  // v = R(1:k-1,1:k-1)\r(1:k-1)
-      R[k - 1 + (int64_t)(k - 1) * ld] /= rv[k - 1];
-      const double rk = R[k - 1 + (int64_t)(k - 1) * ld];
-      for (int i = 0; i < k - 1; ++i) R[i + (int64_t)(k - 1) * ld] = tv[i] * (1.0 - rk);
-      for (int col = k + 1; col < n; ++col) {
-        const double ds = sv[col - k - 1] - R[k - 1 + (int64_t)col * ld];
-        for (int i = 0; i < k - 1; ++i) R[i + (int64_t)col * ld] += tv[i] / rv[k - 1] * ds;
-        R[k - 1 + (int64_t)col * ld] /= rv[k - 1];
-      }
-    }
-    // swap k-th and (k+1)-th columns; update inverse row norms (id.m:201-204)
-    {
-      int t = jpvt[k - 1];
-      jpvt[k - 1] = jpvt[k];
-      jpvt[k] = t;
-      for (int row = 0; row < rows; ++row) {
-        double a = R[row + (int64_t)(k - 1) * ld];
-        R[row + (int64_t)(k - 1) * ld] = R[row + (int64_t)k * ld];
-        R[row + (int64_t)k * ld] = a;
-      }
-    }
-    if (k > 1) {
-      trisolve(R, ld, k - 1, R + (int64_t)(k - 1) * ld, tv);
-      const double rkk = R[k - 1 + (int64_t)(k - 1) * ld];
-      for (int i = 0; i < k - 1; ++i) r2[i] += fabs(tv[i] / rkk) * fabs(tv[i] / rkk);
-    }
-    {
-      const double rkk = R[k - 1 + (int64_t)(k - 1) * ld];
-      r2[k - 1] = 1.0 / (rkk * rkk);
-    }
-    // Sherman-Morrison (id.m:207-208)
-    u[k - 1] -= 1.0;
-    for (int col = k; col < n; ++col) {
-      const double a = R[k - 1 + (int64_t)col * ld] / (1.0 + u[k - 1]);
-      for (int i = 0; i < k; ++i) R[i + (int64_t)col * ld] -= u[i] * a;
-    }
-    // rank reduction (id.m:211-229)
-    double rmin = INFINITY;
-    int imin = 0;
-    for (int i = 0; i < k; ++i) {
-      const double v = 1.0 / sqrt(r2[i]);
-      if (v < rmin) {
-        rmin = v;
-        imin = i;
-      }
-    }
-    if (rmin > tol) continue;
-    if (imin < k - 1) {
-      int t = jpvt[imin];
-      jpvt[imin] = jpvt[k - 1];
-      jpvt[k - 1] = t;
-      swap_retri(R, ld, imin, k);
-      for (int col = k; col < n; ++col) {
-        double a = R[imin + (int64_t)col * ld];
-        R[imin + (int64_t)col * ld] = R[k - 1 + (int64_t)col * ld];
-        R[k - 1 + (int64_t)col * ld] = a;
-      }
-      double a = r2[imin];
-      r2[imin] = r2[k - 1];
-      r2[k - 1] = a;
-    }
-    for (int j = 0; j <= n - k; ++j) c2[j] = 0.0;
-    if (k > 1) {
-      trisolve(R, ld, k - 1, R + (int64_t)(k - 1) * ld, tv);
-      const double rkk = R[k - 1 + (int64_t)(k - 1) * ld];
-      for (int i = 0; i < k - 1; ++i) r2[i] -= fabs(tv[i] / rkk) * fabs(tv[i] / rkk);
-    }
-    k -= 1;
-    trisolve(R, ld, k, R + (int64_t)k * ld, tv);  // r = R(1:k,1:k)\R(1:k,k+1)
-    for (int i = 0; i < k; ++i) R[i + (int64_t)k * ld] = tv[i];
-    for (int col = k + 1; col < n; ++col)
-      for (int i = 0; i < k; ++i) R[i + (int64_t)col * ld] += tv[i] * R[k + (int64_t)col * ld];
-    rows = k;
-    if (k == 0) break;
-  }
-  *niter_out = niter;
-  *capped = (!conv && k > 0 && niter >= kRrqrCap) ? 1 : 0;
-  return k;
 }
 
 __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
@@ -430,7 +166,7 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
   }
   const int nrep = a.symm_n ? 2 : 1;
   const int npr = (t.flags & 1) ? (ip.two_sided ? 2 * P.npxy : P.npxy) : 0;
-  const int m = nrep * m1 + npr;
+  const int m = a.Aexp ? t.ncand : nrep * m1 + npr;
   const int mn = min(m, n);
 
   // ---- (2) TSQR: fold row panels of K into R0 (n x n upper triangular)
@@ -442,7 +178,9 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
     rd.type = 3;
     rd.q = -1;
     rd.wmul = 0.0;
-    if (rho < m1) {
+    if (a.Aexp) {
+      // explicit matrix: rows read below
+    } else if (rho < m1) {
       rd.type = 0;
       rd.q = cand[rho];
     } else if (a.symm_n && rho < 2 * m1) {
@@ -460,7 +198,11 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
         rd.y[k] = P.pxy_shift ? pk + P.pxy_shift[pr * d + k] * t.l[k] + t.ctr[k] : pk * t.l[k] + t.ctr[k];
       }
     }
-    for (int c = wid; c < n; c += kWarps) Pn[(int64_t)c * 32 + lane] = row_entry(P, ip, rd, slf[c]);
+    if (a.Aexp) {
+      for (int c = wid; c < n; c += kWarps) Pn[(int64_t)c * 32 + lane] = rho < m ? a.Aexp[rho + c * a.lda] : 0.0;
+    } else {
+      for (int c = wid; c < n; c += kWarps) Pn[(int64_t)c * 32 + lane] = row_entry(P, ip, rd, slf[c]);
+    }
     __syncthreads();
     for (int j = 0; j < n; ++j) {
       if (wid == 0) {
@@ -510,7 +252,8 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
     ArgMax am{-1.0, n};
     for (int c = i + tid; c < n; c += kThreads) am = better(am, ArgMax{vn1[c], c});
     am = block_argmax(am, red_am);
-    const int pvt = am.i;
+    // a NaN partial norm (non-finite input) leaves the sentinel index: stay in range
+    const int pvt = (am.i >= i && am.i < n) ? am.i : i;
     if (pvt != i) {
       for (int row = tid; row < n; row += kThreads) {
         const double tmp = R[row + (int64_t)pvt * n];
@@ -581,6 +324,14 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
     }
     __syncthreads();
   }
+
+  // The reflectors are stored below the diagonal (as xGEQP3 does); the RRQR
+  // update reads R as the reference's upper-trapezoidal matrix, so clear them.
+  for (int64_t e = tid; e < (int64_t)n * n; e += kThreads) {
+    const int row = (int)(e % n), col = (int)(e / n);
+    if (row > col) R[e] = 0.0;
+  }
+  __syncthreads();
 
   // ---- (4) rank by precision and by the rank cap (id.m:106-113)
   if (tid == 0) {

@@ -145,11 +145,12 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
       if (tid == 0) {
         AM bm = red[0];
         for (int w = 1; w < kWarps; ++w) bm = amax(bm, red[w]);
-        s_piv = bm.i;
-        piv[j] = bm.i;
+        const int pv0 = (bm.i >= j && bm.i < r) ? bm.i : j;
+        s_piv = pv0;
+        piv[j] = pv0;
       }
       __syncthreads();
-      const int pv = s_piv;
+      const int pv = (s_piv >= j && s_piv < r) ? s_piv : j;   // NaN column: keep the row
       if (pv != j)
         for (int col = tid; col < n; col += kThreads) {
           const double tmp = K[k + j + (int64_t)col * n];

@@ -18,6 +18,8 @@ struct CompressArgs {
   int symm_n;          // 1: compress [A(nbr,slf); A(slf,nbr)'; Kpxy] (symm 'n')
   double Tmax;
   int64_t rrqr_iter;   // < 0: unlimited
+  const double* Aexp;  // explicit m x n matrix (flam_id); rows are generated from points when null
+  int64_t lda;
 };
 
 size_t compress_smem_bytes(int n);

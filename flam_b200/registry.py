@@ -27,6 +27,19 @@ KERNELS = {"laplace2d": 0, "laplace2d_dl": 1, "laplace3d": 2, "gaussian": 3, "ma
 PROXIES = {"none": 0, "ring": 1, "sphere": 2, "annulus": 3}
 
 
+def _array(a, fortran=False):
+    """Keep CUDA tensors as they are (device pointers); make host data float64 NumPy."""
+    if type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False):
+        return a
+    return np.asfortranarray(a, dtype=np.float64) if fortran else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+
 class Kernel:
     """Registry matrix; stands where the reference takes the handle ``A``."""
 
@@ -37,14 +50,12 @@ class Kernel:
         self.scale = float(scale)
         self.dval = float(dval)
         self.param = float(param)
-        self.weights = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
-        self.normals = None if normals is None else np.asfortranarray(normals, dtype=np.float64)
+        self.weights = None if weights is None else _array(weights)
+        self.normals = None if normals is None else _array(normals, fortran=True)
 
-    def c_struct(self, weights=None, normals=None):
-        w = self.weights if weights is None else weights
-        n = self.normals if normals is None else normals
-        return _lib.FlamKernel(KERNELS[self.kind], self.scale, self.dval, self.param,
-                               None if w is None else w.ctypes.data, None if n is None else n.ctypes.data)
+    def c_struct(self):
+        return _lib.FlamKernel(KERNELS[self.kind], self.scale, self.dval, self.param, _ptr(self.weights),
+                               _ptr(self.normals))
 
 
 class Proxy:

@@ -101,6 +101,7 @@ typedef struct {
   int stop;              /* stop after this many levels; < 0 means Inf    (rskelf.m:119) */
   int verb;              /* 1: print the per-level table                  (rskelf.m:120) */
   void* stream;          /* cudaStream_t the handle runs on (NULL: default stream) */
+  int profile;           /* 1: time every launch with CUDA events (see flam_profile) */
 } flam_opts;
 
 typedef struct flam_factor flam_factor;
@@ -118,6 +119,13 @@ FLAM_API flam_status flam_rskelf(const double* x, int d, int64_t N, const flam_k
  * ext is d x 2 or NULL.   core/hypoct.m:51-171 */
 FLAM_API flam_status flam_hypoct(const double* x, int d, int64_t N, double occ, int lvlmax, const double* ext,
                                  void* stream, flam_factor** T);
+
+/* [sk, rd, T] = id(A, rank_or_tol, Tmax, rrqr_iter) on the device for an
+ * explicit m x n matrix (leading dimension lda, host or device memory).
+ * Outputs (host): *k, perm (n entries: sk = perm[0:k], rd = perm[k:n]),
+ * T (k x (n-k), leading dimension k) and *niter.  core/id.m:44-248 */
+FLAM_API flam_status flam_id(const double* A, int64_t m, int64_t n, int64_t lda, double rank_or_tol, double Tmax,
+                             int64_t rrqr_iter, int64_t* k, int64_t* perm, double* T, int64_t* niter);
 
 /* Many independent problems in one pipeline: instance i has N[i] points at
  * x + d * (N[0] + ... + N[i-1]) and matrix A[i].  Every step of the
@@ -181,6 +189,20 @@ FLAM_API flam_status flam_factor_export(const flam_factor* F, int inst, int64_t 
 FLAM_API flam_status flam_level_stats(const flam_factor* F, int inst, int* nrows, int64_t* rows);
 
 FLAM_API void flam_factor_free(flam_factor* F);
+
+/* Launch accounting of a handle (factorization and every sv/mv call since the
+ * last reset): device time per kernel family from CUDA events on the handle's
+ * stream, and the algorithmic work those launches did (flops of the
+ * reference's dense operations on each box, bytes of factor and X traffic). */
+typedef struct {
+  int64_t launches;                       /* all kernels this library launched */
+  int64_t n_compress, n_elim, n_sweep;    /* launches of each hot kernel */
+  double t_compress, t_elim, t_sweep;     /* seconds (0 unless profiling is on) */
+  double flop_compress, flop_elim, flop_sweep;
+  double byte_sweep;
+} flam_prof;
+
+FLAM_API flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset);
 
 /* Message of the last failed call on this thread ("FLAM:<fn>:<id>: text"). */
 FLAM_API const char* flam_last_error(void);

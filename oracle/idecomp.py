@@ -7,9 +7,13 @@ LAPACK routines the reference reaches through MATLAB built-ins are called
 through SciPy: ``qr(A,0)`` with three outputs is xGEQP3 (``scipy.linalg.qr``
 with ``pivoting=True``), the unpivoted row reduction is xGEQRF, the
 triangular ``\\`` is xTRTRS.  ``qrupdate`` (used only to re-triangularise R11
-after swapping two of its columns, id.m:134,217) is restated as a fresh QR of
-the swapped R11: every quantity the loop reads from R11 (inverse row norms,
-``R11\\r`` products, T) is invariant under the row-sign freedom of that QR.
+after swapping two of its columns, id.m:134,217) is restated with Givens
+rotations: the spike the swap leaves in column i is cleared bottom-up, then the
+subdiagonal it leaves behind top-down (qrupdate's own rotation signs are not
+pinned by any reference test).  In the tolerance mode every quantity the loop
+reads from R11 (inverse row norms, ``R11\\r`` products, T) is invariant under
+the row signs of R; the fixed-rank branch (id.m:168-198) is not, because it
+sets ``R(k+1,k+1) = sqrt(c2(1))`` whatever sign the reflection produced.
 """
 import math
 import warnings
@@ -24,15 +28,41 @@ def _tri_solve(R, b):
     return sl.solve_triangular(R, b, lower=False, check_finite=False)
 
 
+def _rot(a, b):
+    if b == 0.0:
+        return 1.0, 0.0
+    r = math.hypot(a, b)
+    return a / r, b / r
+
+
 def _swap_r11(R, i, k):
     """Swap columns i and k-1 of R[:k,:k] and re-triangularise (id.m:134,217)."""
-    R11 = R[:k, :k].copy()
-    R11[:, [i, k - 1]] = R11[:, [k - 1, i]]
-    R[:k, :k] = sl.qr(R11, mode="r", check_finite=False)[0]
+    R[:k, [i, k - 1]] = R[:k, [k - 1, i]]
+    for row in range(k - 1, i, -1):              # spike in column i, bottom-up
+        c, s = _rot(R[row - 1, i], R[row, i])
+        a, b = R[row - 1, i:k].copy(), R[row, i:k].copy()
+        R[row - 1, i:k] = c * a + s * b
+        R[row, i:k] = -s * a + c * b
+        R[row, i] = 0.0
+    for col in range(i + 1, k - 1):              # subdiagonal left behind, top-down
+        c, s = _rot(R[col, col], R[col + 1, col])
+        a, b = R[col, col:k].copy(), R[col + 1, col:k].copy()
+        R[col, col:k] = c * a + s * b
+        R[col + 1, col:k] = -s * a + c * b
+        R[col + 1, col] = 0.0
 
 
 def id_(A, rank_or_tol, Tmax=2.0, rrqr_iter=math.inf):
     """core/id.m:44-248 (the ``fixed`` argument is not on the rskelf path)."""
+    st = _id_qr(A, rank_or_tol, Tmax, rrqr_iter)
+    if st[0] == "done":
+        return st[1]
+    _, R, p, k, tol, n = st
+    return _id_rrqr(R, p, k, tol, n, Tmax, rrqr_iter)
+
+
+def _id_qr(A, rank_or_tol, Tmax=2.0, rrqr_iter=math.inf):
+    """id.m:44-114: argument checks, pivoted QR, rank, T stored in R."""
     if Tmax is None:
         Tmax = 2.0
     if rrqr_iter is None:
@@ -47,8 +77,7 @@ def id_(A, rank_or_tol, Tmax=2.0, rrqr_iter=math.inf):
     m, n = A.shape
     niter = 0
     if m == 0 or n == 0:                                   # id.m:64-68
-        return (np.zeros(0, np.int64), np.arange(n, dtype=np.int64),
-                np.zeros((0, n)), 0)
+        return ("done", (np.zeros(0, np.int64), np.arange(n, dtype=np.int64), np.zeros((0, n)), 0))
     tol = math.fmod(rank_or_tol, 1.0)                      # id.m:71
     kmax = int(math.floor(rank_or_tol))                    # id.m:72
     if kmax == 0 or kmax > n:
@@ -69,7 +98,16 @@ def id_(A, rank_or_tol, Tmax=2.0, rrqr_iter=math.inf):
     k = min(k, kmax)                                       # id.m:113
     if k > 0 and k < n:
         R[:k, k:] = _tri_solve(R[:k, :k], R[:k, k:])       # id.m:114
+    return ("rrqr", R, p, k, tol, n)
 
+
+def _id_rrqr(R, p, k, tol, n, Tmax, rrqr_iter):
+    """id.m:116-240: RRQR refinement of (R with T stored, p, k) and the outputs."""
+    if Tmax is None:
+        Tmax = 2.0
+    if rrqr_iter is None:
+        rrqr_iter = math.inf
+    niter = 0
     # RRQR refinement (id.m:117-236)
     if not math.isinf(Tmax) and rrqr_iter > 0 and 0 < k < n:
         f2 = Tmax ** 2
