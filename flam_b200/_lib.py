@@ -19,7 +19,7 @@ STATUS = {
 
 # every symbol include/flam.h declares
 EXPORTS = (
-    "flam_opts_default", "flam_hypoct", "flam_id", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
+    "flam_opts_default", "flam_hypoct", "flam_id", "flam_id_noalloc", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
     "flam_factor_info", "flam_tree_export", "flam_tree_perm", "flam_factor_sizes", "flam_factor_export",
     "flam_level_stats", "flam_factor_free", "flam_profile", "flam_last_error", "flam_version",
 )
@@ -87,6 +87,9 @@ def lib():
     L.flam_id.argtypes = [P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64, i64p, i64p, dp,
                           i64p]
     L.flam_id.restype = C.c_int
+    L.flam_id_noalloc.argtypes = [P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64, P, P, P,
+                                  P, P]
+    L.flam_id_noalloc.restype = C.c_int
     L.flam_rskelf_batched.argtypes = [C.c_int, P, C.c_int, i64p, C.POINTER(FlamKernel), C.c_double, C.c_double,
                                       C.POINTER(FlamProxy), C.POINTER(FlamOpts), C.POINTER(P)]
     L.flam_rskelf_batched.restype = C.c_int

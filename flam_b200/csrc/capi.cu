@@ -1165,6 +1165,9 @@ flam_status guard(Fn&& fn) {
 }
 
 }  // namespace
+
+void set_last_error(const char* msg) { g_err = msg; }
+
 }  // namespace flam
 
 extern "C" {

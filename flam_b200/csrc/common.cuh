@@ -108,6 +108,9 @@ struct FacDesc {
   int32_t k, r;
 };
 
+// Record the message flam_last_error() returns on this thread (defined with the C ABI).
+void set_last_error(const char* msg);
+
 // Factorization status word bits (device -> host).
 enum StatusBits { ST_NOT_SPD = 1, ST_SINGULAR = 2, ST_RRQR_CAP = 4 };
 

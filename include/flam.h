@@ -127,6 +127,28 @@ FLAM_API flam_status flam_hypoct(const double* x, int d, int64_t N, double occ, 
 FLAM_API flam_status flam_id(const double* A, int64_t m, int64_t n, int64_t lda, double rank_or_tol, double Tmax,
                              int64_t rrqr_iter, int64_t* k, int64_t* perm, double* T, int64_t* niter);
 
+/* Column limit of flam_id_noalloc. */
+#define FLAM_ID_NOALLOC_NMAX 128
+
+/* flam_id without device allocation -- no counterpart in the reference.
+ * For callers that cannot allocate device memory (a MEX/oct gateway running
+ * inside a MATLAB or Octave session whose GPU memory manager owns the device
+ * heap, a thread that must not enter cudaMalloc/cudaFree): the caller passes
+ * DEVICE pointers for the m x n matrix A (leading dimension lda) and for every
+ * output -- *k, perm (n entries, sk = perm[0:k], rd = perm[k:n]), T (room for
+ * n*n/4 + 1 doubles; written k x (n-k), leading dimension k) and *niter (may be
+ * NULL) -- and the work runs asynchronously on `stream` (NULL: legacy default
+ * stream).  Scratch is a 64 KiB array compiled into the library, resident on
+ * every GPU that loads it until the process exits; n is limited to
+ * FLAM_ID_NOALLOC_NMAX (larger n returns FLAM_ERR_ARG).  The first call on a
+ * device looks up that array's address with the device current; make that
+ * first call before any stream capture.  All calls share the array: calls that
+ * overlap on one GPU race and must be serialised by the caller.
+ * Same algorithm and results as flam_id (core/id.m:44-248). */
+FLAM_API flam_status flam_id_noalloc(const double* A, int64_t m, int64_t n, int64_t lda, double rank_or_tol,
+                                     double Tmax, int64_t rrqr_iter, int64_t* k, int64_t* perm, double* T,
+                                     int64_t* niter, void* stream);
+
 /* Many independent problems in one pipeline: instance i has N[i] points at
  * x + d * (N[0] + ... + N[i-1]) and matrix A[i].  Every step of the
  * factorization runs all instances' boxes of the matching level in one launch.
