@@ -21,7 +21,7 @@ STATUS = {
 EXPORTS = (
     "flam_opts_default", "flam_hypoct", "flam_id", "flam_id_noalloc", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
     "flam_factor_info", "flam_tree_export", "flam_tree_perm", "flam_factor_sizes", "flam_factor_export",
-    "flam_level_stats", "flam_factor_free", "flam_profile", "flam_last_error", "flam_version",
+    "flam_level_stats", "flam_factor_free", "flam_workspace_release", "flam_profile", "flam_last_error", "flam_version",
 )
 
 
@@ -111,6 +111,8 @@ def lib():
     L.flam_level_stats.restype = C.c_int
     L.flam_profile.argtypes = [P, C.POINTER(FlamProf), C.c_int]
     L.flam_profile.restype = C.c_int
+    L.flam_workspace_release.argtypes = []
+    L.flam_workspace_release.restype = None
     L.flam_factor_free.argtypes = [P]
     L.flam_factor_free.restype = None
     L.flam_last_error.argtypes = []

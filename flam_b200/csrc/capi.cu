@@ -16,7 +16,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -94,6 +96,17 @@ struct DBuf {
     p = nullptr;
     n = cap = 0;
   }
+  // size c without keeping the old contents (work buffers)
+  void ensure(int64_t c, cudaStream_t s) {
+    if (c > cap) {
+      if (p) CK(cudaFreeAsync(p, s));
+      p = nullptr;
+      cap = 0;
+      n = 0;
+      reserve(c, s);
+    }
+    n = c;
+  }
   int64_t bytes() const { return cap * (int64_t)sizeof(T); }
 };
 
@@ -123,6 +136,45 @@ struct StepDev {
 struct LevelStat {
   int64_t lvl, nblk, nrem1, nrem2;
 };
+
+// Work buffers of the factorization steps and the sweeps, kept per (device,
+// stream) for the life of the process and only ever grown: after the first
+// call no step allocates device memory (a fresh pool allocation of the
+// multi-hundred-MB sweep buffer can cost the driver hundreds of ms).  Calls on
+// one stream run in order, so they can share it; flam_workspace_release()
+// returns the memory.
+struct Workspace {
+  DBuf<int64_t> cpool;
+  DBuf<double> tpool, scratch, mpool[2], W, tmp;
+  DBuf<int32_t> permpool, status;
+  DBuf<CompressTask> ctask;
+  DBuf<ElimTask> etask;
+  DBuf<ChildBlock> chb;
+  DBuf<CopySeg> segs, csegs;
+  DBuf<CompressOut> cout;
+  void release(cudaStream_t s) {
+    for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp}) b->release(s);
+    cpool.release(s);
+    permpool.release(s);
+    status.release(s);
+    ctask.release(s);
+    etask.release(s);
+    chb.release(s);
+    segs.release(s);
+    csegs.release(s);
+    cout.release(s);
+  }
+};
+
+std::mutex g_ws_mu;
+std::map<std::pair<int, cudaStream_t>, std::unique_ptr<Workspace>> g_ws;
+
+Workspace& workspace(int dev, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  auto& w = g_ws[{dev, s}];
+  if (!w) w.reset(new Workspace());
+  return *w;
+}
 
 }  // namespace
 }  // namespace flam
@@ -165,8 +217,20 @@ struct flam_factor {
   int64_t warn = 0;
   bool profile = false;
   mutable flam_prof prof{};
+  mutable cudaEvent_t pend[2] = {nullptr, nullptr};   // sweep timing not yet read
+  mutable bool has_pend = false;
+  void resolve_pending() const {
+    if (!has_pend) return;
+    float ms = 0;
+    if (cudaEventSynchronize(pend[1]) == cudaSuccess && cudaEventElapsedTime(&ms, pend[0], pend[1]) == cudaSuccess)
+      prof.t_sweep += ms * 1e-3;
+    cudaEventDestroy(pend[0]);
+    cudaEventDestroy(pend[1]);
+    has_pend = false;
+  }
 
   ~flam_factor() {
+    resolve_pending();
     if (!s && !x.p) return;
     cudaStream_t st = s;
     x.release(st);
@@ -572,15 +636,20 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   const int maxsteps = *std::max_element(F.nlvl.begin(), F.nlvl.end());
   const int64_t stop = o.stop < 0 ? INT64_MAX : o.stop;
 
-  DBuf<int64_t> cpool;
-  DBuf<double> tpool, scratch, mpool[2];
-  DBuf<int32_t> permpool, status;
-  DBuf<CompressTask> ctask;
-  DBuf<ElimTask> etask;
-  DBuf<ChildBlock> chb;
-  DBuf<CopySeg> segs;
-  DBuf<CompressOut> cout;
-  status.resize(1, s);
+  Workspace& ws = workspace(F.dev, s);
+  auto& cpool = ws.cpool;
+  auto& tpool = ws.tpool;
+  auto& scratch = ws.scratch;
+  auto& mpool = ws.mpool;
+  auto& permpool = ws.permpool;
+  auto& status = ws.status;
+  auto& ctask = ws.ctask;
+  auto& etask = ws.etask;
+  auto& chb = ws.chb;
+  auto& segs = ws.segs;
+  auto& csegs = ws.csegs;
+  auto& cout = ws.cout;
+  status.ensure(1, s);
   CK(cudaMemsetAsync(status.p, 0, sizeof(int32_t), s));
   Problem P;
   P.d = F.d;
@@ -595,10 +664,11 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   int64_t fpool_top = 0, ppool_top = 0;
   const bool prof = F.profile;
   const bool prof_print = std::getenv("FLAM_PROFILE") != nullptr;
-  cudaEvent_t pe[4] = {};
+  // per-step CUDA events around the compress and elimination launches; resolved
+  // after the last step so that profiling adds no synchronisation
+  std::vector<cudaEvent_t> step_ev;
+  cudaEvent_t* pe = nullptr;
 
-  if (prof)
-    for (auto& e : pe) CK(cudaEventCreate(&e));
   for (int step = 0; step < maxsteps && step < stop; ++step) {
     // ---- boxes of this step: level nlvl_i - step of each instance
     std::vector<int32_t> boxes;
@@ -663,9 +733,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       ncand[q] = n;
       ctop += n;
     }
-    cpool.resize(std::max<int64_t>(ctop, 1), s);
+    cpool.ensure(std::max<int64_t>(ctop, 1), s);
     // ---- tasks
     std::vector<CompressTask> ct(nb);
+    std::vector<int64_t> elim_scr(nb, -1);
     int64_t ttop = 0, ptop = 0, stop_s = 0;
     int nmax_small = 0;
     for (int q = 0; q < nb; ++q) {
@@ -688,24 +759,43 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       ttop += (nslf[q] * nslf[q]) / 4 + 1;
       t.perm_off = ptop;
       ptop += nslf[q];
-      if (nslf[q] > kSmemN) {
-        t.scr_off = stop_s;
-        stop_s += std::max(compress_scratch_doubles((int)nslf[q]), elim_scratch_doubles((int)nslf[q]));
-      } else {
-        t.scr_off = -1;
-        nmax_small = std::max<int>(nmax_small, (int)nslf[q]);
+      t.out_idx = q;
+      // work matrices: shared memory when they fit, else a per-box slot of global scratch
+      // shared by the compress and elimination kernels of this step
+      const int n = (int)nslf[q];
+      const bool tc = n <= kTcMaxN;
+      const bool c_glob = tc ? compress_tc_smem_bytes(n) > kTcSmemMax : n > kSmemN;
+      const bool e_glob = n > kSmemN;
+      t.scr_off = -1;
+      elim_scr[q] = -1;
+      if (c_glob || e_glob) {
+        const int64_t slot = std::max(tc ? compress_tc_doubles(n) : compress_scratch_doubles(n), elim_scratch_doubles(n));
+        if (c_glob) t.scr_off = stop_s;
+        if (e_glob) elim_scr[q] = stop_s;
+        stop_s += slot;
       }
+      if (!tc && !c_glob) nmax_small = std::max<int>(nmax_small, n);
     }
-    tpool.resize(std::max<int64_t>(ttop, 1), s);
-    permpool.resize(std::max<int64_t>(ptop, 1), s);
-    scratch.resize(std::max<int64_t>(stop_s, 1), s);
+    tpool.ensure(std::max<int64_t>(ttop, 1), s);
+    permpool.ensure(std::max<int64_t>(ptop, 1), s);
+    scratch.ensure(std::max<int64_t>(stop_s, 1), s);
     segs.upload(sg, s);
     launch_gather_ids(F.ipool.p, F.ipool.p, segs.p, (int)sg.size(), s);
-    DBuf<CopySeg> csegs;
     csegs.upload(cs, s);
     launch_gather_ids(F.ipool.p, cpool.p, csegs.p, (int)cs.size(), s);
-    ctask.upload(ct, s);
-    cout.resize(nb, s);
+    // group the boxes by kernel shape: thread-per-column blocks of 32..1024 threads,
+    // and the per-column kernel for n > kTcMaxN
+    auto kkey = [&](int q) {
+      const int n = (int)nslf[q];
+      return n <= kTcMaxN ? compress_tc_threads(n) * 8 + compress_tc_group(n) : 0;
+    };
+    std::vector<int> ord(nb);
+    for (int q = 0; q < nb; ++q) ord[q] = q;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return kkey(x) < kkey(y); });
+    std::vector<CompressTask> cts(nb);
+    for (int q = 0; q < nb; ++q) cts[q] = ct[ord[q]];
+    ctask.upload(cts, s);
+    cout.ensure(nb, s);
     CompressArgs ca{};
     ca.P = P;
     ca.tasks = ctask.p;
@@ -724,12 +814,34 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ca.lda = 0;
     F.prof.launches += 2 + 1;  // two id gathers, compress
     F.prof.n_compress += 1;
-    if (prof) CK(cudaEventRecord(pe[0], s));
-    launch_compress(ca, nb, compress_smem_bytes(nmax_small), s);
+    if (prof) {
+      const size_t base = step_ev.size();
+      step_ev.resize(base + 4);
+      for (size_t e = base; e < base + 4; ++e) CK(cudaEventCreate(&step_ev[e]));
+      pe = step_ev.data() + base;
+      CK(cudaEventRecord(pe[0], s));
+    }
+    for (int b0 = 0; b0 < nb;) {
+      const int key = kkey(ord[b0]);
+      int b1 = b0;
+      size_t sm = 16;
+      while (b1 < nb && kkey(ord[b1]) == key) {
+        if (key > 0 && cts[b1].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(cts[b1].n));
+        ++b1;
+      }
+      CompressArgs cb = ca;
+      cb.tasks = ctask.p + b0;
+      if (key == 0)
+        launch_compress(cb, b1 - b0, compress_smem_bytes(nmax_small), s);
+      else
+        launch_compress_tc(cb, b1 - b0, key / 8, key % 8, sm, s);
+      F.prof.launches += 1;
+      b0 = b1;
+    }
+    F.prof.launches -= 1;
     CK(cudaGetLastError());
     if (prof) CK(cudaEventRecord(pe[1], s));
     auto co = download(cout.p, nb, s);
-    csegs.release(s);
 
     // ---- elimination plan
     std::vector<ElimTask> et(nb);
@@ -750,7 +862,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       t.inst = F.binst[b];
       t.ch_first = ch_first[q];
       t.nch = nchv[q];
-      t.scr_off = ct[q].scr_off;
+      t.scr_off = elim_scr[q];
       if (n <= kSmemN) nmax_e = std::max(nmax_e, n);
       t.M_out = mtop;
       mtop += r > 0 ? (int64_t)k * k : (int64_t)n * n;
@@ -785,7 +897,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     F.fpool.n = fpool_top;
     F.ppool.reserve(std::max<int64_t>(ppool_top, 1), s);
     F.ppool.n = ppool_top;
-    mpool[cur].resize(std::max<int64_t>(mtop, 1), s);
+    mpool[cur].ensure(std::max<int64_t>(mtop, 1), s);
     etask.upload(et, s);
     chb.upload(ch, s);
     ElimArgs ea{};
@@ -818,16 +930,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     if (prof) CK(cudaEventRecord(pe[2], s));
     launch_eliminate(ea, nb, elim_smem_bytes(nmax_e), s);
     CK(cudaGetLastError());
-    if (prof) {
-      CK(cudaEventRecord(pe[3], s));
-      CK(cudaEventSynchronize(pe[3]));
-      float tc = 0, tel = 0;
-      CK(cudaEventElapsedTime(&tc, pe[0], pe[1]));
-      CK(cudaEventElapsedTime(&tel, pe[2], pe[3]));
-      F.prof.t_compress += tc * 1e-3;
-      F.prof.t_elim += tel * 1e-3;
-    }
+    if (prof) CK(cudaEventRecord(pe[3], s));
     if (prof && prof_print) {
+      CK(cudaEventSynchronize(pe[3]));
       float tc = 0, tel = 0;
       CK(cudaEventElapsedTime(&tc, pe[0], pe[1]));
       CK(cudaEventElapsedTime(&tel, pe[2], pe[3]));
@@ -886,17 +991,14 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   F.t_factor = ms * 1e-3;
   CK(cudaEventDestroy(e0));
   CK(cudaEventDestroy(e1));
-  if (prof)
-    for (auto& e : pe) CK(cudaEventDestroy(e));
-  for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1]}) b->release(s);
-  cpool.release(s);
-  permpool.release(s);
-  status.release(s);
-  ctask.release(s);
-  etask.release(s);
-  chb.release(s);
-  segs.release(s);
-  cout.release(s);
+  for (size_t e = 0; e + 3 < step_ev.size(); e += 4) {
+    float tc = 0, tel = 0;
+    CK(cudaEventElapsedTime(&tc, step_ev[e], step_ev[e + 1]));
+    CK(cudaEventElapsedTime(&tel, step_ev[e + 2], step_ev[e + 3]));
+    F.prof.t_compress += tc * 1e-3;
+    F.prof.t_elim += tel * 1e-3;
+  }
+  for (auto& e : step_ev) CK(cudaEventDestroy(e));
   CK(cudaStreamSynchronize(s));
   if (st & ST_NOT_SPD)
     fail(FLAM_ERR_NOT_SPD, "FLAM:rskelf:notPosDef: a redundant block is not positive definite (chol failed)");
@@ -1072,15 +1174,17 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   const bool dev = is_device_ptr(X);
   double* Xd = X;
   int64_t ld = ldx;
-  DBuf<double> tmp, W;
+  Workspace& ws = workspace(F->dev, s);
+  auto& tmp = ws.tmp;
+  auto& W = ws.W;
   if (!dev) {
-    tmp.resize(N * nrhs, s);
+    tmp.ensure(N * nrhs, s);
     CK(cudaMemcpy2DAsync(tmp.p, sizeof(double) * N, X, sizeof(double) * ldx, sizeof(double) * N, nrhs,
                          cudaMemcpyHostToDevice, s));
     Xd = tmp.p;
     ld = N;
   }
-  W.resize(N * nrhs, s);
+  W.ensure(N * nrhs, s);
   mark(1);
   launch_to_pointmajor(Xd, ld, N, (int)nrhs, W.p, s);
   mark(2);
@@ -1094,28 +1198,23 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   a.trans = t;
   a.symm = F->symm;
   const int ns = (int)F->steps.size();
-  cudaEvent_t ev[2] = {};
+  // profiling: one event pair around the sweep launches (back to back on the
+  // stream), read when the profile is next asked for -- no synchronisation here
+  F->resolve_pending();
   if (F->profile) {
-    CK(cudaEventCreate(&ev[0]));
-    CK(cudaEventCreate(&ev[1]));
+    CK(cudaEventCreate(&F->pend[0]));
+    CK(cudaEventCreate(&F->pend[1]));
+    CK(cudaEventRecord(F->pend[0], s));
   }
   auto sweep = [&](int q) {
     const StepDev& sd = F->steps[q];
     a.fac = sd.fac.p;
     if (sd.nfac == 0) return;
-    if (F->profile) CK(cudaEventRecord(ev[0], s));
     launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
     F->prof.launches += 1;
     F->prof.n_sweep += 1;
     F->prof.flop_sweep += sd.flop_per_rhs * (double)nrhs;
     F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)nrhs;
-    if (F->profile) {
-      CK(cudaEventRecord(ev[1], s));
-      CK(cudaEventSynchronize(ev[1]));
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-      F->prof.t_sweep += ms * 1e-3;
-    }
   };
   F->prof.launches += 2;  // layout changes
   a.op = solve ? 0 : 2;
@@ -1123,8 +1222,8 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   a.op = solve ? 1 : 3;
   for (int q = ns - 1; q >= 0; --q) sweep(q);
   if (F->profile) {
-    CK(cudaEventDestroy(ev[0]));
-    CK(cudaEventDestroy(ev[1]));
+    CK(cudaEventRecord(F->pend[1], s));
+    F->has_pend = true;
   }
   CK(cudaGetLastError());
   mark(3);
@@ -1133,8 +1232,6 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   if (!dev)
     CK(cudaMemcpy2DAsync(X, sizeof(double) * ldx, tmp.p, sizeof(double) * N, sizeof(double) * N, nrhs,
                          cudaMemcpyDeviceToHost, s));
-  W.release(s);
-  tmp.release(s);
   mark(5);
   if (!dev) CK(cudaStreamSynchronize(s));
   if (pp) {
@@ -1514,9 +1611,24 @@ flam_status flam_level_stats(const flam_factor* F, int inst, int* nrows, int64_t
 
 void flam_factor_free(flam_factor* F) { delete F; }
 
+void flam_workspace_release(void) {
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (auto& kv : g_ws) {
+    cudaSetDevice(kv.first.first);
+    cudaStreamSynchronize(kv.first.second);
+    kv.second->release(kv.first.second);
+    cudaStreamSynchronize(kv.first.second);
+  }
+  g_ws.clear();
+  cudaSetDevice(cur);
+}
+
 flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset) {
   return guard([&] {
     if (!F) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: NULL factor");
+    F->resolve_pending();
     if (out) *out = F->prof;
     if (reset) F->prof = flam_prof{};
     return FLAM_OK;

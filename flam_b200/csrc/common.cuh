@@ -64,7 +64,7 @@ struct CompressTask {
   int32_t box;
   int32_t inst;
   int32_t flags;     // bit0: compress with proxy (lvl > 2); bit1: filter candidates
-  int32_t pad;
+  int32_t out_idx;   // slot of this box in the CompressOut array
   double ctr[kMaxDim];
   double l[kMaxDim];
 };

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
   const int n = t.n;
   const int d = P.d;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  CompressOut* out = a.out + blockIdx.x;
+  CompressOut* out = a.out + t.out_idx;
   int64_t* slf = a.ipool + t.slf_off;
   int64_t* cand = a.cpool + t.cand_off;
   if (n == 0) {
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kThreads) k_compress(CompressArgs a) {
         int niter = 0, capped = 0;
         const double tol = a.rel_tol * fabs(R[0]);
         // aux scratch: the panel region is free after the TSQR (32 n doubles)
-        const int kk = rrqr_serial(R, n, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, Pn, &niter, &capped);
+        const int kk = rrqr_serial(R, 1, n, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, Pn, &niter, &capped);
         s_k = kk;
         s_niter = niter;
         s_cap = capped;

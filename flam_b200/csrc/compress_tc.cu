@@ -1,0 +1,454 @@
+// K4+K5+K6, thread-per-column form: fused proxy filter, block assembly and
+// interpolative decomposition, one CTA per box, one thread per column of the
+// box's block K = [A(nbr,slf); A(slf,nbr)'; Kpxy] (rskelf/rskelf.m:201-213,
+// core/id.m:59-240).
+//
+// TSQR.  Rows of K are generated B at a time; thread c keeps its column's B
+// panel entries in registers and R (n x n, upper triangular, row-major) lives
+// in shared memory (global scratch for large n).  Reflector j annihilates the
+// panel's column j into R(j,j); the thread owning column j+1 applies
+// reflector j to its column and immediately forms reflector j+1, so each
+// reflector costs one barrier and every other thread's work is a register
+// dot product and update with the reflector broadcast from shared memory.
+//
+// Pivoted QR of R0 (xLAQP2 rule: first maximum of the partial column norms,
+// sqrt(eps) downdating threshold, min(m, n) steps), then rank, T = R11\R12 and
+// the RRQR refinement (rrqr.cuh) exactly as the per-column kernel in
+// compress.cu, whose results this kernel reproduces up to rounding.
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "rrqr.cuh"
+
+namespace flam {
+namespace {
+
+struct AMx {
+  double v;
+  int i;
+};
+
+__device__ __forceinline__ AMx amx_better(AMx a, AMx b) {
+  if (b.v > a.v || (b.v == a.v && b.i < a.i)) return b;  // first maximum, like IDAMAX
+  return a;
+}
+
+template <int B>
+struct Stage {
+  double y[B][kMaxDim];  // proxy point of a proxy row
+  double wmul[B];        // proxy multiplier (0: use the column's weight)
+  int64_t q[B];          // neighbour point of an A(nbr,slf) / A(slf,nbr)' row
+  int type[B];           // 0 A(nbr,slf), 1 A(slf,nbr)', 2 proxy, 3 zero
+};
+
+// Sum over the G consecutive lanes that share a column (G divides 32).
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned gmask) {
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(gmask, v, o);
+  return v;
+}
+
+// Reflector j of the current panel, formed by the G threads that own column j
+// (thread g holds panel rows g*B .. g*B+B-1): annihilates the panel's column j
+// into R(j,j) (DLARFG conventions).
+template <int B, int G>
+__device__ __forceinline__ void reflect_col(double (&p)[B], double* R, int ld, int j, int g, unsigned gmask,
+                                            double* vb, double* tau_out) {
+  const double al = R[(int64_t)j * ld + j];
+  double sig = 0.0;
+#pragma unroll
+  for (int i = 0; i < B; ++i) sig += p[i] * p[i];
+  sig = group_sum<G>(sig, gmask);
+  double tau = 0.0;
+  if (sig != 0.0) {
+    const double be = -copysign(sqrt(al * al + sig), al);
+    tau = (be - al) / be;
+    const double scal = 1.0 / (al - be);
+#pragma unroll
+    for (int i = 0; i < B; ++i) vb[g * B + i] = p[i] * scal;
+    __syncwarp(gmask);
+    if (g == 0) R[(int64_t)j * ld + j] = be;
+  }
+  if (g == 0) *tau_out = tau;
+}
+
+__device__ __forceinline__ double entry_of(const Problem& P, const InstParams& ip, int type, int64_t q,
+                                           const double* y, double wmul, int64_t sc) {
+  switch (type) {
+    case 0:
+      return aentry(P, ip, q, sc);
+    case 1:
+      return aentry(P, ip, sc, q);
+    case 2: {
+      const double v = ip.pscale * keval(ip.pkernel, ip.pparam, P.d, y, P.x + sc * P.d, nullptr);
+      if (wmul != 0.0) return v * wmul;
+      return ip.has_w ? v * P.w[sc] : v;
+    }
+    default:
+      return 0.0;
+  }
+}
+
+template <int B, int G>
+__global__ void __launch_bounds__(B == 32 ? 512 : 1024) k_compress_tc(CompressArgs a) {
+  constexpr int PH = B * G;  // panel height
+  extern __shared__ __align__(16) double smem[];
+  __shared__ Stage<PH> st;
+  __shared__ double vbuf[2][PH];
+  __shared__ double tau2[2];
+  __shared__ AMx red_am[32];
+  __shared__ double red_d[32];
+  __shared__ int s_cnt[32];
+  __shared__ int s_k, s_ktol, s_niter, s_cap, s_need;
+
+  const CompressTask t = a.tasks[blockIdx.x];
+  const Problem& P = a.P;
+  const InstParams ip = P.ip[t.inst];
+  const int n = t.n, d = P.d;
+  const int NT = blockDim.x, nw = NT >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int c = tid;  // the column this thread owns (if c < n)
+  CompressOut* out = a.out + t.out_idx;
+  int64_t* slf = a.ipool + t.slf_off;
+  int64_t* cand = a.cpool + t.cand_off;
+  if (n == 0) {
+    if (tid == 0) *out = CompressOut{0, 0, 0, 0};
+    return;
+  }
+  const int ld = n | 1;  // odd row stride: column accesses of R hit distinct banks
+  double* R = (t.scr_off >= 0) ? a.scratch + t.scr_off : smem;   // n x ld, row-major
+  double* vn1 = R + (int64_t)n * ld;
+  double* vn2 = vn1 + n;
+  double* aux = vn2 + n;                                         // 6n (RRQR), reused for ids
+  int* jpvt = reinterpret_cast<int*>(aux + 6 * (int64_t)n);
+
+  // ---- (1) neighbour filter (pxyfun's nbr selection), stable compaction in place
+  int m1 = t.ncand;
+  if (t.flags & 2) {
+    int total = 0;
+    for (int c0 = 0; c0 < t.ncand; c0 += NT) {
+      const int ci = c0 + tid;
+      int64_t q = -1;
+      bool keep = false;
+      if (ci < t.ncand) {
+        q = cand[ci];
+        const double* xq = P.x + q * d;
+        if (ip.pkind == P_ANNULUS) {
+          double mx = 0.0;
+          for (int k = 0; k < d; ++k) mx = fmax(mx, __ddiv_rn(fabs(__dsub_rn(xq[k], t.ctr[k])), t.l[k]));
+          keep = mx < 1.5;
+        } else {
+          double s = 0.0;
+          for (int k = 0; k < d; ++k) {
+            const double z = __ddiv_rn(__dsub_rn(xq[k], t.ctr[k]), t.l[k]);
+            s = __dadd_rn(s, __dmul_rn(z, z));
+          }
+          keep = s < 2.25;
+        }
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) s_cnt[wid] = __popc(bal);
+      __syncthreads();
+      int pre = total, tot = 0;
+      for (int w = 0; w < nw; ++w) {
+        if (w < wid) pre += s_cnt[w];
+        tot += s_cnt[w];
+      }
+      if (keep) cand[pre + __popc(bal & ((1u << lane) - 1u))] = q;
+      total += tot;
+      __syncthreads();
+    }
+    m1 = total;
+  }
+  const int nrep = a.symm_n ? 2 : 1;
+  const int npr = (t.flags & 1) ? (ip.two_sided ? 2 * P.npxy : P.npxy) : 0;
+  const int m = a.Aexp ? t.ncand : nrep * m1 + npr;
+  const int mn = min(m, n);
+
+  // ---- (2) TSQR: fold PH-row panels of K into R0; G threads per column
+  for (int64_t e = tid; e < (int64_t)n * ld; e += NT) R[e] = 0.0;
+  const int col = tid / G, g = tid % G;
+  const unsigned gmask = (G == 1) ? (1u << lane) : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  const int64_t sc = col < n ? slf[col] : 0;
+  __syncthreads();
+  double p[B];
+  for (int p0 = 0; p0 < m; p0 += PH) {
+    if (!a.Aexp && tid < PH) {
+      const int rho = p0 + tid;
+      int ty = 3;
+      int64_t q = -1;
+      double wm = 0.0;
+      if (rho < m1) {
+        ty = 0;
+        q = cand[rho];
+      } else if (a.symm_n && rho < 2 * m1) {
+        ty = 1;
+        q = cand[rho - m1];
+      } else if (rho < m) {
+        int pr = rho - nrep * m1;
+        ty = 2;
+        if (ip.two_sided && pr >= P.npxy) {
+          pr -= P.npxy;
+          wm = ip.wbar;
+        }
+        for (int k = 0; k < d; ++k) {
+          const double pk = P.pxy_pts[pr * d + k];
+          st.y[tid][k] = P.pxy_shift ? pk + P.pxy_shift[pr * d + k] * t.l[k] + t.ctr[k] : pk * t.l[k] + t.ctr[k];
+        }
+      }
+      st.type[tid] = ty;
+      st.q[tid] = q;
+      st.wmul[tid] = wm;
+    }
+    __syncthreads();
+    if (col < n) {
+      const int r0 = p0 + g * B;
+      if (a.Aexp) {
+#pragma unroll
+        for (int i = 0; i < B; ++i) p[i] = (r0 + i < m) ? a.Aexp[(r0 + i) + (int64_t)col * a.lda] : 0.0;
+      } else {
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+          const int s = g * B + i;
+          p[i] = entry_of(P, ip, st.type[s], st.q[s], st.y[s], st.wmul[s], sc);
+        }
+      }
+    }
+    // reflector 0 of this panel, formed by its owners
+    if (col == 0) reflect_col<B, G>(p, R, ld, 0, g, gmask, vbuf[0], &tau2[0]);
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+      const int b = j & 1;
+      const double tau = tau2[b];
+      if (tau != 0.0 && col > j && col < n) {
+        const double* v = vbuf[b] + g * B;
+        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+#pragma unroll
+        for (int i = 0; i < B; i += 4) {
+          w0 += v[i] * p[i];
+          w1 += v[i + 1] * p[i + 1];
+          w2 += v[i + 2] * p[i + 2];
+          w3 += v[i + 3] * p[i + 3];
+        }
+        const double rjc = R[(int64_t)j * ld + col];
+        const double tw = tau * (rjc + group_sum<G>((w0 + w1) + (w2 + w3), gmask));
+        if (g == 0) R[(int64_t)j * ld + col] = rjc - tw;
+#pragma unroll
+        for (int i = 0; i < B; ++i) p[i] -= tw * v[i];
+      }
+      if (col == j + 1 && col < n) reflect_col<B, G>(p, R, ld, j + 1, g, gmask, vbuf[b ^ 1], &tau2[b ^ 1]);
+      __syncthreads();
+    }
+  }
+
+  // ---- (3) column-pivoted QR of R0 (xLAQP2) for min(m, n) steps
+  if (c < n) {
+    double s = 0.0;
+    for (int r = 0; r < n; ++r) s += R[(int64_t)r * ld + c] * R[(int64_t)r * ld + c];
+    vn1[c] = vn2[c] = sqrt(s);
+    jpvt[c] = c;
+  }
+  __syncthreads();
+  const double tol3z = 1.0536712127723509e-08;  // sqrt(2^-53), LAPACK's dlamch('Epsilon')
+  for (int i = 0; i < mn; ++i) {
+    AMx am{-1.0, n};
+    if (c >= i && c < n) am = AMx{vn1[c], c};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      AMx o2{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+      am = amx_better(am, o2);
+    }
+    if (lane == 0) red_am[wid] = am;
+    __syncthreads();
+    AMx bm = red_am[0];
+    for (int w = 1; w < nw; ++w) bm = amx_better(bm, red_am[w]);
+    const int pvt = (bm.i >= i && bm.i < n) ? bm.i : i;   // NaN norms keep the column
+    __syncthreads();
+    if (pvt != i) {
+      for (int r = tid; r < n; r += NT) {
+        const double tmp = R[(int64_t)r * ld + pvt];
+        R[(int64_t)r * ld + pvt] = R[(int64_t)r * ld + i];
+        R[(int64_t)r * ld + i] = tmp;
+      }
+      if (tid == 0) {
+        const int tj = jpvt[pvt];
+        jpvt[pvt] = jpvt[i];
+        jpvt[i] = tj;
+        vn1[pvt] = vn1[i];
+        vn2[pvt] = vn2[i];
+      }
+    }
+    __syncthreads();
+    if (wid == 0) {  // DLARFG on column i, rows i..m-1
+      double s = 0.0;
+      if (i + 1 < m)
+        for (int r = i + 1 + lane; r < n; r += 32) s += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + i];
+      s = warp_sum(s);
+      double tau = 0.0;
+      if (s != 0.0) {
+        const double al = R[(int64_t)i * ld + i];
+        const double be = -copysign(hypot(al, sqrt(s)), al);
+        tau = (be - al) / be;
+        const double scal = 1.0 / (al - be);
+        for (int r = i + 1 + lane; r < n; r += 32) R[(int64_t)r * ld + i] *= scal;
+        __syncwarp();
+        if (lane == 0) R[(int64_t)i * ld + i] = be;
+      }
+      if (lane == 0) tau2[0] = tau;
+    }
+    __syncthreads();
+    const double tau = tau2[0];
+    if (c > i && c < n) {
+      if (tau != 0.0) {
+        double w0 = R[(int64_t)i * ld + c], w1 = 0.0;
+        int r = i + 1;
+        for (; r + 1 < n; r += 2) {
+          w0 += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + c];
+          w1 += R[(int64_t)(r + 1) * ld + i] * R[(int64_t)(r + 1) * ld + c];
+        }
+        if (r < n) w0 += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + c];
+        const double tw = tau * (w0 + w1);
+        R[(int64_t)i * ld + c] -= tw;
+        for (int rr = i + 1; rr < n; ++rr) R[(int64_t)rr * ld + c] -= tw * R[(int64_t)rr * ld + i];
+      }
+      if (vn1[c] != 0.0) {  // partial norm downdate (xLAQP2)
+        double temp = fabs(R[(int64_t)i * ld + c]) / vn1[c];
+        temp = fmax(1.0 - temp * temp, 0.0);
+        const double q = vn1[c] / vn2[c];
+        if (temp * q * q <= tol3z) {
+          if (i + 1 < m) {
+            double s = 0.0;
+            for (int rr = i + 1; rr < n; ++rr) s += R[(int64_t)rr * ld + c] * R[(int64_t)rr * ld + c];
+            vn1[c] = vn2[c] = sqrt(s);
+          } else {
+            vn1[c] = vn2[c] = 0.0;
+          }
+        } else {
+          vn1[c] *= sqrt(temp);
+        }
+      }
+    }
+    // the next step's pivot reduction starts with a barrier-separated exchange
+  }
+  __syncthreads();
+  // clear the reflectors below the diagonal (the RRQR update reads R as upper trapezoidal)
+  if (c < n)
+    for (int r = c + 1; r < n; ++r) R[(int64_t)r * ld + c] = 0.0;
+
+  // ---- (4) rank (id.m:106-113)
+  if (tid == 0) {
+    const double tol = a.rel_tol * fabs(R[0]);
+    int kt = 0;
+    if (m > 0)
+      for (int i = 0; i < mn; ++i) kt += fabs(R[(int64_t)i * ld + i]) > tol;
+    int kmax = a.kmax;
+    if (kmax == 0 || kmax > n) kmax = n;
+    s_ktol = kt;
+    s_k = min(kt, kmax);
+    s_niter = 0;
+    s_cap = 0;
+  }
+  __syncthreads();
+  int k = s_k;
+  const int ktol = s_ktol;
+
+  // ---- (5) T = R11 \ R12 (id.m:114), one column per thread
+  if (k > 0 && k < n && m > 0 && c >= k && c < n) {
+    for (int i = k - 1; i >= 0; --i) {
+      double v = R[(int64_t)i * ld + c];
+      for (int j = i + 1; j < k; ++j) v -= R[(int64_t)i * ld + j] * R[(int64_t)j * ld + c];
+      R[(int64_t)i * ld + c] = v / R[(int64_t)i * ld + i];
+    }
+  }
+  __syncthreads();
+
+  // ---- (6) RRQR refinement (id.m:117-236), only when some |T| > Tmax (or R22 is present)
+  if (m > 0 && !isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
+    double mx = 0.0;
+    if (c >= k && c < n)
+      for (int i = 0; i < k; ++i) mx = fmax(mx, R[(int64_t)i * ld + c] * R[(int64_t)i * ld + c]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red_d[wid] = mx;
+    __syncthreads();
+    if (tid == 0) {
+      double bm = 0.0;
+      for (int w = 0; w < nw; ++w) bm = fmax(bm, red_d[w]);
+      s_need = (ktol > k || bm > a.Tmax * a.Tmax) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_need) {
+      if (tid == 0) {
+        int niter = 0, capped = 0;
+        const double tol = a.rel_tol * fabs(R[0]);
+        const int kk = rrqr_serial(R, ld, 1, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped);
+        s_k = kk;
+        s_niter = niter;
+        s_cap = capped;
+      }
+      __syncthreads();
+      k = s_k;
+    }
+  }
+
+  // ---- (7) outputs: [sk rd] order of slf, local permutation, T
+  const int r = n - k;
+  int* perm_out = a.permpool + t.perm_off;
+  const bool keep_order = (r == 0) || (m == 0);   // rskelf.m:216 (no factor) / id.m:64-68 (empty block)
+  int64_t* tmp_ids = reinterpret_cast<int64_t*>(aux);
+  for (int q = tid; q < n; q += NT) tmp_ids[q] = slf[q];
+  __syncthreads();
+  for (int q = tid; q < n; q += NT) {
+    const int src = keep_order ? q : jpvt[q];
+    perm_out[q] = src;
+    slf[q] = tmp_ids[src];
+  }
+  if (r > 0 && k > 0 && c >= k && c < n) {
+    double* T = a.tpool + t.T_off;
+    for (int i = 0; i < k; ++i) T[i + (int64_t)(c - k) * k] = R[(int64_t)i * ld + c];
+  }
+  if (tid == 0) *out = CompressOut{k, m, s_niter, s_cap ? (int)ST_RRQR_CAP : 0};
+}
+
+template <int B, int G>
+void launch_b(const CompressArgs& a, int ntask, int nt, size_t smem, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_compress_tc<B, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  k_compress_tc<B, G><<<ntask, nt, smem, s>>>(a);
+}
+
+}  // namespace
+
+int64_t compress_tc_doubles(int n) { return (int64_t)n * (n | 1) + 8 * (int64_t)n + n / 2 + 2; }
+
+size_t compress_tc_smem_bytes(int n) { return sizeof(double) * (size_t)compress_tc_doubles(n); }
+
+// Threads per column: 4 for n <= 64, 2 for n <= 256, else 1 (512 threads at most
+// with 32 panel rows per thread; 1024 threads with 16 rows for n > 512).
+int compress_tc_group(int n) { return n <= 64 ? 4 : (n <= 256 ? 2 : 1); }
+
+int compress_tc_threads(int n) {
+  int cols = 32;
+  while (cols < n) cols <<= 1;
+  const int nt = cols * compress_tc_group(n);
+  return nt < 128 && compress_tc_group(n) == 4 ? 128 : nt;
+}
+
+void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int g, size_t smem, cudaStream_t s) {
+  if (ntask <= 0) return;
+  if (nt > 512)
+    launch_b<16, 1>(a, ntask, nt, smem, s);
+  else if (g == 4)
+    launch_b<32, 4>(a, ntask, nt, smem, s);
+  else if (g == 2)
+    launch_b<32, 2>(a, ntask, nt, smem, s);
+  else
+    launch_b<32, 1>(a, ntask, nt, smem, s);
+}
+
+}  // namespace flam

@@ -67,35 +67,55 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
     return a.m_in[ch[c].M_off + ploc[i] + (int64_t)ploc[j] * kc];
   };
 
+  // 2D loops use a fixed 32 x 8 thread tile: lane = row within a 32-row block
+  // (consecutive column-major addresses), warp = column within an 8-column block;
+  // no index is divided and every lane has work once a block has 32 rows.
+  const int tr = lane, tcol = wid;
   if (r == 0) {  // no compression: the box keeps its whole modified block (rskelf.m:216)
     double* Mo = a.m_out + t.M_out;
-    for (int64_t e = tid; e < (int64_t)n * n; e += kThreads) Mo[e] = mval((int)(e % n), (int)(e / n));
+    for (int j = tcol; j < n; j += kWarps)
+      for (int i = tr; i < n; i += 32) Mo[i + (int64_t)j * n] = mval(i, j);
     return;
   }
 
   // K = A(slf,slf) + M in [sk rd] order
-  for (int64_t e = tid; e < (int64_t)n * n; e += kThreads) {
-    const int i = (int)(e % n), j = (int)(e / n);
-    K[e] = aentry(P, ip, slf[i], slf[j]) + mval(i, j);
+  for (int j = tcol; j < n; j += kWarps) {
+    const int64_t sj = slf[j];
+    for (int i = tr; i < n; i += 32) K[i + (int64_t)j * n] = aentry(P, ip, slf[i], sj) + mval(i, j);
   }
   __syncthreads();
 
   const double* T = a.tpool + t.T_off;  // k x r, ld k
   if (k > 0) {
     // K(rd,:) = K(rd,:) - T' K(sk,:)      (T.' for 's': identical for real data)
-    for (int64_t e = tid; e < (int64_t)r * n; e += kThreads) {
-      const int i = (int)(e % r), col = (int)(e / r);
-      double s = 0.0;
-      for (int b = 0; b < k; ++b) s += T[b + (int64_t)i * k] * K[b + (int64_t)col * n];
-      K[k + i + (int64_t)col * n] -= s;
+    for (int col = tcol; col < n; col += kWarps) {
+      const double* Kc = K + (int64_t)col * n;
+      for (int i = tr; i < r; i += 32) {
+        const double* Ti = T + (int64_t)i * k;
+        double s0 = 0.0, s1 = 0.0;
+        int b = 0;
+        for (; b + 1 < k; b += 2) {
+          s0 += Ti[b] * Kc[b];
+          s1 += Ti[b + 1] * Kc[b + 1];
+        }
+        if (b < k) s0 += Ti[b] * Kc[b];
+        K[k + i + (int64_t)col * n] -= s0 + s1;
+      }
     }
     __syncthreads();
     // K(:,rd) = K(:,rd) - K(:,sk) T
-    for (int64_t e = tid; e < (int64_t)n * r; e += kThreads) {
-      const int row = (int)(e % n), j = (int)(e / n);
-      double s = 0.0;
-      for (int b = 0; b < k; ++b) s += K[row + (int64_t)b * n] * T[b + (int64_t)j * k];
-      K[row + (int64_t)(k + j) * n] -= s;
+    for (int j = tcol; j < r; j += kWarps) {
+      const double* Tj = T + (int64_t)j * k;
+      for (int row = tr; row < n; row += 32) {
+        double s0 = 0.0, s1 = 0.0;
+        int b = 0;
+        for (; b + 1 < k; b += 2) {
+          s0 += K[row + (int64_t)b * n] * Tj[b];
+          s1 += K[row + (int64_t)(b + 1) * n] * Tj[b + 1];
+        }
+        if (b < k) s0 += K[row + (int64_t)b * n] * Tj[b];
+        K[row + (int64_t)(k + j) * n] -= s0 + s1;
+      }
     }
     __syncthreads();
   }
@@ -114,10 +134,9 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
       for (int q = j + 1 + tid; q < r; q += kThreads) Kr[q + (int64_t)j * n] /= lj;
       if (tid == 0) Kr[j + (int64_t)j * n] = lj;
       __syncthreads();
-      const int rem = r - j - 1;
-      for (int64_t e = tid; e < (int64_t)rem * rem; e += kThreads) {
-        const int q = j + 1 + (int)(e % rem), c = j + 1 + (int)(e / rem);
-        if (q >= c) Kr[q + (int64_t)c * n] -= Kr[q + (int64_t)j * n] * Kr[c + (int64_t)j * n];
+      for (int c = j + 1 + tcol; c < r; c += kWarps) {
+        const double lc = Kr[c + (int64_t)j * n];
+        for (int q = c + tr; q < r; q += 32) Kr[q + (int64_t)c * n] -= Kr[q + (int64_t)j * n] * lc;
       }
       __syncthreads();
     }
@@ -165,10 +184,9 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
         atomicOr(a.status, (int)ST_SINGULAR);
       }
       __syncthreads();
-      const int rem = r - j - 1;
-      for (int64_t e = tid; e < (int64_t)rem * rem; e += kThreads) {
-        const int q = j + 1 + (int)(e % rem), c = j + 1 + (int)(e / rem);
-        Kr[q + (int64_t)c * n] -= Kr[q + (int64_t)j * n] * Kr[j + (int64_t)c * n];
+      for (int c = j + 1 + tcol; c < r; c += kWarps) {
+        const double ujc = Kr[j + (int64_t)c * n];
+        for (int q = j + 1 + tr; q < r; q += 32) Kr[q + (int64_t)c * n] -= Kr[q + (int64_t)j * n] * ujc;
       }
       __syncthreads();
     }
@@ -194,33 +212,28 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
   // M_new = M(sk,sk) - E*G   (E*E' for 'p')
   double* Mo = a.m_out + t.M_out;
   const bool chol = a.symm == 'p';
-  for (int64_t e = tid; e < (int64_t)k * k; e += kThreads) {
-    const int i = (int)(e % k), j = (int)(e / k);
-    double s = 0.0;
-    if (chol)
-      for (int q = 0; q < r; ++q) s += K[i + (int64_t)(k + q) * n] * K[j + (int64_t)(k + q) * n];
-    else
-      for (int q = 0; q < r; ++q) s += K[i + (int64_t)(k + q) * n] * K[k + q + (int64_t)j * n];
-    Mo[e] = mval(i, j) - s;
+  for (int j = tcol; j < k; j += kWarps) {
+    for (int i = tr; i < k; i += 32) {
+      double s = 0.0;
+      if (chol)
+        for (int q = 0; q < r; ++q) s += K[i + (int64_t)(k + q) * n] * K[j + (int64_t)(k + q) * n];
+      else
+        for (int q = 0; q < r; ++q) s += K[i + (int64_t)(k + q) * n] * K[k + q + (int64_t)j * n];
+      Mo[i + (int64_t)j * k] = mval(i, j) - s;
+    }
   }
 
   // store the factor: T | LU (or L) | E | G
   double* F = a.fpool + t.fac_off;
   const int64_t kr = (int64_t)k * r, rr = (int64_t)r * r;
   for (int64_t e = tid; e < kr; e += kThreads) F[e] = T[e];
-  for (int64_t e = tid; e < rr; e += kThreads) {
-    const int i = (int)(e % r), j = (int)(e / r);
-    F[kr + e] = (chol && i < j) ? 0.0 : Kr[i + (int64_t)j * n];
-  }
-  for (int64_t e = tid; e < kr; e += kThreads) {
-    const int i = (int)(e % k), j = (int)(e / k);
-    F[kr + rr + e] = K[i + (int64_t)(k + j) * n];
-  }
+  for (int j = tcol; j < r; j += kWarps)
+    for (int i = tr; i < r; i += 32) F[kr + i + (int64_t)j * r] = (chol && i < j) ? 0.0 : Kr[i + (int64_t)j * n];
+  for (int j = tcol; j < r; j += kWarps)
+    for (int i = tr; i < k; i += 32) F[kr + rr + i + (int64_t)j * k] = K[i + (int64_t)(k + j) * n];
   if (!chol) {
-    for (int64_t e = tid; e < kr; e += kThreads) {
-      const int i = (int)(e % r), j = (int)(e / r);
-      F[2 * kr + rr + e] = K[k + i + (int64_t)j * n];
-    }
+    for (int j = tcol; j < k; j += kWarps)
+      for (int i = tr; i < r; i += 32) F[2 * kr + rr + i + (int64_t)j * r] = K[k + i + (int64_t)j * n];
     if (tid == 0) {  // p from the sequence of interchanges
       int32_t* pp = a.ppool + t.piv_off;
       for (int q = 0; q < r; ++q) pp[q] = q;

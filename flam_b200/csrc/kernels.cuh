@@ -26,6 +26,17 @@ size_t compress_smem_bytes(int n);
 int64_t compress_scratch_doubles(int n);
 void launch_compress(const CompressArgs& a, int ntask, size_t smem, cudaStream_t s);
 
+// Thread-per-column compress (compress_tc.cu) for n <= kTcMaxN: nt threads per box
+// (compress_tc_threads(n)), work arrays of compress_tc_doubles(n) in shared memory
+// when they fit kTcSmemMax, else in the task's global scratch.
+constexpr int kTcMaxN = 1024;
+constexpr size_t kTcSmemMax = 200 * 1024;
+int64_t compress_tc_doubles(int n);
+size_t compress_tc_smem_bytes(int n);
+int compress_tc_threads(int n);
+int compress_tc_group(int n);
+void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int g, size_t smem, cudaStream_t s);
+
 struct ElimArgs {
   Problem P;
   const ElimTask* tasks;

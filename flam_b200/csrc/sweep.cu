@@ -27,102 +27,135 @@
 namespace flam {
 namespace {
 
-// ---- primitives on one right-hand side column held in shared memory with stride ts
-// y(0:r) += sign * A' x(0:k), A k x r (ld k); y(i) pairs with column perm[i] of A
-// when y is held in the permuted order X(rd(p)).
-__device__ __forceinline__ void sub_At_x(double* y, const double* x, const double* A, int k, int r, int ts,
-                                         double sign, const int32_t* perm = nullptr) {
-  for (int i = 0; i < r; ++i) {
-    const double* Ac = A + (int64_t)(perm ? perm[i] : i) * k;
-    double s = 0.0;
-    for (int b = 0; b < k; ++b) s += Ac[b] * x[b * ts];
-    y[i * ts] += sign * s;
+// ---- CTA-cooperative primitives on a tile of kTs right-hand sides held in shared
+// memory, row-major (X[row * kTs + col]); lane = column, warp w takes rows w, w+8, ...
+// A matrix M is read through strides: M(i, j) = M[i * rs + j * cs], so the same
+// routine applies a factor or its transpose.
+constexpr int kTs = 32;
+constexpr int kSw = 8;                 // warps per CTA
+constexpr int kSweepThreads = 32 * kSw;
+
+struct Mat {
+  const double* p;
+  int64_t rs, cs;
+  const int32_t* rmap;  // optional row index map
+  const int32_t* cmap;  // optional column index map
+  __device__ __forceinline__ double at(int i, int j) const {
+    const int ii = rmap ? rmap[i] : i, jj = cmap ? cmap[j] : j;
+    return p[ii * rs + jj * cs];
   }
-}
-// y(0:m) += sign * A x(0:q), A m x q (ld m); x(b) pairs with column perm[b] of A.
-__device__ __forceinline__ void sub_A_x(double* y, const double* x, const double* A, int m, int q, int ts,
-                                        double sign, const int32_t* perm = nullptr) {
-  for (int i = 0; i < m; ++i) {
-    double s = 0.0;
-    for (int b = 0; b < q; ++b) s += A[i + (int64_t)(perm ? perm[b] : b) * m] * x[b * ts];
-    y[i * ts] += sign * s;
-  }
-}
-// triangular solves / products with the r x r factor M (ld r)
-__device__ __forceinline__ void solve_lower(double* x, const double* M, int r, int ts, bool unit) {
-  for (int i = 0; i < r; ++i) {
-    double v = x[i * ts];
-    for (int j = 0; j < i; ++j) v -= M[i + (int64_t)j * r] * x[j * ts];
-    x[i * ts] = unit ? v : v / M[i + (int64_t)i * r];
-  }
-}
-__device__ __forceinline__ void solve_upper(double* x, const double* M, int r, int ts) {
-  for (int i = r - 1; i >= 0; --i) {
-    double v = x[i * ts];
-    for (int j = i + 1; j < r; ++j) v -= M[i + (int64_t)j * r] * x[j * ts];
-    x[i * ts] = v / M[i + (int64_t)i * r];
-  }
-}
-// x = U' \ x (U upper -> U' lower)
-__device__ __forceinline__ void solve_upper_t(double* x, const double* M, int r, int ts) {
-  for (int i = 0; i < r; ++i) {
-    double v = x[i * ts];
-    for (int j = 0; j < i; ++j) v -= M[j + (int64_t)i * r] * x[j * ts];
-    x[i * ts] = v / M[i + (int64_t)i * r];
-  }
-}
-// x = L' \ x (L lower -> L' upper)
-__device__ __forceinline__ void solve_lower_t(double* x, const double* M, int r, int ts, bool unit) {
-  for (int i = r - 1; i >= 0; --i) {
-    double v = x[i * ts];
-    for (int j = i + 1; j < r; ++j) v -= M[j + (int64_t)i * r] * x[j * ts];
-    x[i * ts] = unit ? v : v / M[i + (int64_t)i * r];
-  }
-}
-// x = U x
-__device__ __forceinline__ void mul_upper(double* x, const double* M, int r, int ts) {
-  for (int i = 0; i < r; ++i) {
-    double s = 0.0;
-    for (int j = i; j < r; ++j) s += M[i + (int64_t)j * r] * x[j * ts];
-    x[i * ts] = s;
-  }
-}
-// x = U' x
-__device__ __forceinline__ void mul_upper_t(double* x, const double* M, int r, int ts) {
-  for (int i = r - 1; i >= 0; --i) {
-    double s = 0.0;
-    for (int j = 0; j <= i; ++j) s += M[j + (int64_t)i * r] * x[j * ts];
-    x[i * ts] = s;
-  }
-}
-// x = L x
-__device__ __forceinline__ void mul_lower(double* x, const double* M, int r, int ts, bool unit) {
-  for (int i = r - 1; i >= 0; --i) {
-    double s = unit ? x[i * ts] : M[i + (int64_t)i * r] * x[i * ts];
-    for (int j = 0; j < i; ++j) s += M[i + (int64_t)j * r] * x[j * ts];
-    x[i * ts] = s;
-  }
-}
-// x = L' x
-__device__ __forceinline__ void mul_lower_t(double* x, const double* M, int r, int ts, bool unit) {
-  for (int i = 0; i < r; ++i) {
-    double s = unit ? x[i * ts] : M[i + (int64_t)i * r] * x[i * ts];
-    for (int j = i + 1; j < r; ++j) s += M[j + (int64_t)i * r] * x[j * ts];
-    x[i * ts] = s;
+};
+
+// Y(0:m, :) += sign * A(0:m, 0:q) X(0:q, :)
+__device__ void gemm_acc(double* Y, const double* X, Mat A, int m, int q, double sign) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int i0 = w; i0 < m; i0 += 4 * kSw) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    const int i1 = i0 + kSw, i2 = i0 + 2 * kSw, i3 = i0 + 3 * kSw;
+    for (int b = 0; b < q; ++b) {
+      const double xb = X[b * kTs + lane];
+      s0 += A.at(i0, b) * xb;
+      if (i1 < m) s1 += A.at(i1, b) * xb;
+      if (i2 < m) s2 += A.at(i2, b) * xb;
+      if (i3 < m) s3 += A.at(i3, b) * xb;
+    }
+    Y[i0 * kTs + lane] += sign * s0;
+    if (i1 < m) Y[i1 * kTs + lane] += sign * s1;
+    if (i2 < m) Y[i2 * kTs + lane] += sign * s2;
+    if (i3 < m) Y[i3 * kTs + lane] += sign * s3;
   }
 }
 
-__global__ void k_sweep(SweepArgs a, double* gscr, int64_t slot) {
+// X = M^-1 X for M (r x r) lower triangular in the (i, j) sense of M.at: blocks of kSw rows,
+// the block's rows first take the contribution of the rows already solved (all warps),
+// then warp 0 solves the kSw x kSw diagonal block.
+__device__ void trsm_fwd(double* X, Mat M, int r, bool unit) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int i0 = 0; i0 < r; i0 += kSw) {
+    const int i = i0 + w;
+    if (i < r && i0 > 0) {
+      double s0 = 0.0, s1 = 0.0;
+      int j = 0;
+      for (; j + 1 < i0; j += 2) {
+        s0 += M.at(i, j) * X[j * kTs + lane];
+        s1 += M.at(i, j + 1) * X[(j + 1) * kTs + lane];
+      }
+      if (j < i0) s0 += M.at(i, j) * X[j * kTs + lane];
+      X[i * kTs + lane] -= s0 + s1;
+    }
+    __syncthreads();
+    if (w == 0) {
+      const int i1 = min(i0 + kSw, r);
+      for (int ii = i0; ii < i1; ++ii) {
+        double v = X[ii * kTs + lane];
+        for (int jj = i0; jj < ii; ++jj) v -= M.at(ii, jj) * X[jj * kTs + lane];
+        X[ii * kTs + lane] = unit ? v : v / M.at(ii, ii);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// X = M^-1 X for M upper triangular (backward substitution), same blocking.
+__device__ void trsm_bwd(double* X, Mat M, int r, bool unit) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int i1 = r; i1 > 0; i1 -= kSw) {
+    const int i0 = max(i1 - kSw, 0);
+    const int i = i0 + w;
+    if (i < i1 && i1 < r) {
+      double s0 = 0.0, s1 = 0.0;
+      int j = i1;
+      for (; j + 1 < r; j += 2) {
+        s0 += M.at(i, j) * X[j * kTs + lane];
+        s1 += M.at(i, j + 1) * X[(j + 1) * kTs + lane];
+      }
+      if (j < r) s0 += M.at(i, j) * X[j * kTs + lane];
+      X[i * kTs + lane] -= s0 + s1;
+    }
+    __syncthreads();
+    if (w == 0) {
+      for (int ii = i1 - 1; ii >= i0; --ii) {
+        double v = X[ii * kTs + lane];
+        for (int jj = ii + 1; jj < i1; ++jj) v -= M.at(ii, jj) * X[jj * kTs + lane];
+        X[ii * kTs + lane] = unit ? v : v / M.at(ii, ii);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// X = M X for M triangular (lower: j <= i, upper: j >= i) through the scratch tile Y.
+__device__ void trmm(double* X, double* Y, Mat M, int r, bool lower, bool unit) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int i = w; i < r; i += kSw) {
+    const int j0 = lower ? 0 : i, j1 = lower ? i + 1 : r;
+    double s0 = 0.0, s1 = 0.0;
+    int j = j0;
+    for (; j + 1 < j1; j += 2) {
+      const double m0 = (unit && j == i) ? 1.0 : M.at(i, j);
+      const double m1 = (unit && j + 1 == i) ? 1.0 : M.at(i, j + 1);
+      s0 += m0 * X[j * kTs + lane];
+      s1 += m1 * X[(j + 1) * kTs + lane];
+    }
+    if (j < j1) s0 += ((unit && j == i) ? 1.0 : M.at(i, j)) * X[j * kTs + lane];
+    Y[i * kTs + lane] = s0 + s1;
+  }
+  __syncthreads();
+  for (int i = w; i < r; i += kSw) X[i * kTs + lane] = Y[i * kTs + lane];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(SweepArgs a, double* gscr, int64_t slot) {
   extern __shared__ __align__(16) double smem[];
   const FacDesc f = a.fac[blockIdx.x];
   const int k = f.k, r = f.r;
-  const int ts = blockDim.x;
-  const int c = blockIdx.y * ts + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c0 = blockIdx.y * kTs;
+  const int c = c0 + lane;
   const bool act = c < a.nrhs;
   double* xs = gscr ? gscr + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * slot : smem;
-  double* xr = xs + (int64_t)k * ts;
-  double* ys = xs + threadIdx.x;  // this thread's column
-  double* yr = xr + threadIdx.x;
+  double* xr = xs + (int64_t)k * kTs;
+  double* yt = xr + (int64_t)r * kTs;   // scratch tile for the triangular products
   const int64_t* sk = a.ipool + f.sk_off;
   const int64_t* rd = sk + k;
   const double* T = a.fpool + f.T_off;
@@ -131,69 +164,86 @@ __global__ void k_sweep(SweepArgs a, double* gscr, int64_t slot) {
   const double* G = a.fpool + f.G_off;
   const int32_t* p = a.ppool + f.piv_off;
   const bool lu = a.symm != 'p';
-  // gather with p for the steps that read X(rd(p))
   const bool gather_p = lu && ((a.op == 0 && a.trans == 0) || (a.op == 2 && a.trans == 1));
   const bool scatter_p = lu && ((a.op == 1 && a.trans == 1) || (a.op == 3 && a.trans == 0));
+  for (int b = w; b < k; b += kSw) xs[b * kTs + lane] = act ? a.X[sk[b] * a.ldx + c] : 0.0;
+  for (int i = w; i < r; i += kSw) xr[i * kTs + lane] = act ? a.X[rd[gather_p ? p[i] : i] * a.ldx + c] : 0.0;
+  __syncthreads();
+  // factor views (column-major storage): A(i, j) = A[i + j * ld]; transposes swap strides
+  const Mat Tn{T, 1, k, nullptr, nullptr}, Tt{T, k, 1, nullptr, nullptr};
+  const Mat Ln{LU, 1, r, nullptr, nullptr}, Lt{LU, r, 1, nullptr, nullptr};
+  const Mat En{E, 1, k, nullptr, nullptr}, Et{E, k, 1, nullptr, nullptr};
+  const Mat Gn{G, 1, r, nullptr, nullptr}, Gt{G, r, 1, nullptr, nullptr};
+  // T' X(sk) and T X(rd) with X(rd) held in the permuted order X(rd(p))
+  const Mat Ttp{T, k, 1, gather_p || scatter_p ? p : nullptr, nullptr};
+  const Mat Tnp{T, 1, k, nullptr, gather_p || scatter_p ? p : nullptr};
+  const int tr = a.trans;
+  switch (a.op) {
+    case 0:  // sv upward
+      gemm_acc(xr, xs, gather_p ? Ttp : Tt, r, k, -1.0);
+      __syncthreads();
+      if (!lu) {
+        trsm_fwd(xr, Ln, r, false);
+        gemm_acc(xs, xr, En, k, r, -1.0);
+      } else if (!tr) {
+        trsm_fwd(xr, Ln, r, true);
+        gemm_acc(xs, xr, En, k, r, -1.0);
+      } else {
+        trsm_fwd(xr, Lt, r, false);      // U' \ x
+        gemm_acc(xs, xr, Gt, k, r, -1.0);
+      }
+      break;
+    case 1:  // sv downward
+      if (!lu) {
+        gemm_acc(xr, xs, Et, r, k, -1.0);
+        __syncthreads();
+        trsm_bwd(xr, Lt, r, false);      // L' \ x
+      } else if (!tr) {
+        gemm_acc(xr, xs, Gn, r, k, -1.0);
+        __syncthreads();
+        trsm_bwd(xr, Ln, r, false);      // U \ x
+      } else {
+        gemm_acc(xr, xs, Et, r, k, -1.0);
+        __syncthreads();
+        trsm_bwd(xr, Lt, r, true);       // L' \ x, unit
+      }
+      gemm_acc(xs, xr, scatter_p ? Tnp : Tn, k, r, -1.0);
+      break;
+    case 2:  // mv upward
+      gemm_acc(xs, xr, gather_p ? Tnp : Tn, k, r, 1.0);
+      __syncthreads();
+      if (!lu) {
+        trmm(xr, yt, Lt, r, false, false);   // L' x
+        gemm_acc(xr, xs, Et, r, k, 1.0);
+      } else if (!tr) {
+        trmm(xr, yt, Ln, r, false, false);   // U x
+        gemm_acc(xr, xs, Gn, r, k, 1.0);
+      } else {
+        trmm(xr, yt, Lt, r, false, true);    // L' x, unit
+        gemm_acc(xr, xs, Et, r, k, 1.0);
+      }
+      break;
+    default:  // mv downward
+      if (!lu) {
+        gemm_acc(xs, xr, En, k, r, 1.0);
+        __syncthreads();
+        trmm(xr, yt, Ln, r, true, false);    // L x
+      } else if (!tr) {
+        gemm_acc(xs, xr, En, k, r, 1.0);
+        __syncthreads();
+        trmm(xr, yt, Ln, r, true, true);     // L x, unit
+      } else {
+        gemm_acc(xs, xr, Gt, k, r, 1.0);
+        __syncthreads();
+        trmm(xr, yt, Lt, r, true, false);    // U' x
+      }
+      gemm_acc(xr, xs, scatter_p ? Ttp : Tt, r, k, 1.0);
+      break;
+  }
+  __syncthreads();
   if (act) {
-    for (int b = 0; b < k; ++b) ys[b * ts] = a.X[sk[b] * a.ldx + c];
-    for (int i = 0; i < r; ++i) yr[i * ts] = a.X[rd[gather_p ? p[i] : i] * a.ldx + c];
-    const int tr = a.trans;
-    switch (a.op) {
-      case 0:  // sv upward
-        sub_At_x(yr, ys, T, k, r, ts, -1.0, gather_p ? p : nullptr);
-        if (!lu) {
-          solve_lower(yr, LU, r, ts, false);
-          sub_A_x(ys, yr, E, k, r, ts, -1.0);
-        } else if (!tr) {
-          solve_lower(yr, LU, r, ts, true);
-          sub_A_x(ys, yr, E, k, r, ts, -1.0);
-        } else {
-          solve_upper_t(yr, LU, r, ts);
-          sub_At_x(ys, yr, G, r, k, ts, -1.0);
-        }
-        break;
-      case 1:  // sv downward
-        if (!lu) {
-          sub_At_x(yr, ys, E, k, r, ts, -1.0);
-          solve_lower_t(yr, LU, r, ts, false);
-        } else if (!tr) {
-          sub_A_x(yr, ys, G, r, k, ts, -1.0);
-          solve_upper(yr, LU, r, ts);
-        } else {
-          sub_At_x(yr, ys, E, k, r, ts, -1.0);
-          solve_lower_t(yr, LU, r, ts, true);
-        }
-        sub_A_x(ys, yr, T, k, r, ts, -1.0, scatter_p ? p : nullptr);
-        break;
-      case 2:  // mv upward
-        sub_A_x(ys, yr, T, k, r, ts, 1.0, gather_p ? p : nullptr);
-        if (!lu) {
-          mul_lower_t(yr, LU, r, ts, false);
-          sub_At_x(yr, ys, E, k, r, ts, 1.0);
-        } else if (!tr) {
-          mul_upper(yr, LU, r, ts);
-          sub_A_x(yr, ys, G, r, k, ts, 1.0);
-        } else {
-          mul_lower_t(yr, LU, r, ts, true);
-          sub_At_x(yr, ys, E, k, r, ts, 1.0);
-        }
-        break;
-      default:  // mv downward
-        if (!lu) {
-          sub_A_x(ys, yr, E, k, r, ts, 1.0);
-          mul_lower(yr, LU, r, ts, false);
-        } else if (!tr) {
-          sub_A_x(ys, yr, E, k, r, ts, 1.0);
-          mul_lower(yr, LU, r, ts, true);
-        } else {
-          sub_At_x(ys, yr, G, r, k, ts, 1.0);
-          mul_upper_t(yr, LU, r, ts);
-        }
-        sub_At_x(yr, ys, T, k, r, ts, 1.0, scatter_p ? p : nullptr);
-        break;
-    }
-    for (int b = 0; b < k; ++b) a.X[sk[b] * a.ldx + c] = ys[b * ts];
-    for (int i = 0; i < r; ++i) a.X[rd[scatter_p ? p[i] : i] * a.ldx + c] = yr[i * ts];
+    for (int b = w; b < k; b += kSw) a.X[sk[b] * a.ldx + c] = xs[b * kTs + lane];
+    for (int i = w; i < r; i += kSw) a.X[rd[scatter_p ? p[i] : i] * a.ldx + c] = xr[i * kTs + lane];
   }
 }
 
@@ -242,22 +292,22 @@ __global__ void k_from_pm(const double* W, int64_t N, int nrhs, double* X, int64
 
 void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t s) {
   if (nfac <= 0 || a.nrhs <= 0) return;
-  int ts = a.nrhs >= 128 ? 128 : ((a.nrhs + 31) / 32) * 32;
-  size_t need = sizeof(double) * (size_t)(kmax + rmax) * ts;
+  // X(sk), X(rd) and a scratch tile for the triangular products, kTs columns each
+  const int64_t slot = (int64_t)(kmax + 2 * rmax) * kTs;
+  const size_t need = sizeof(double) * (size_t)slot;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  dim3 g(nfac, (a.nrhs + ts - 1) / ts);
+  dim3 g(nfac, (a.nrhs + kTs - 1) / kTs);
   if (need <= 160 * 1024) {
-    k_sweep<<<g, ts, need, s>>>(a, nullptr, 0);
+    k_sweep<<<g, kSweepThreads, need, s>>>(a, nullptr, 0);
   } else {
     // rows of huge factors do not fit in shared memory: stage them in global scratch
-    const int64_t slot = (int64_t)(kmax + rmax) * ts;
     double* scr = nullptr;
     cudaMallocAsync(&scr, sizeof(double) * slot * g.x * g.y, s);
-    k_sweep<<<g, ts, 0, s>>>(a, scr, slot);
+    k_sweep<<<g, kSweepThreads, 0, s>>>(a, scr, slot);
     cudaFreeAsync(scr, s);
   }
 }

@@ -212,6 +212,12 @@ FLAM_API flam_status flam_level_stats(const flam_factor* F, int inst, int* nrows
 
 FLAM_API void flam_factor_free(flam_factor* F);
 
+/* The library keeps the work buffers of factorizations and sweeps per
+ * (device, stream) and reuses them (they only grow), so steady-state calls
+ * allocate no device memory.  This returns that memory to the device pool;
+ * call it with no library work in flight (it synchronises those streams). */
+FLAM_API void flam_workspace_release(void);
+
 /* Launch accounting of a handle (factorization and every sv/mv call since the
  * last reset): device time per kernel family from CUDA events on the handle's
  * stream, and the algorithmic work those launches did (flops of the

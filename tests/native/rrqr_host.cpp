@@ -4,5 +4,5 @@
 
 extern "C" int flam_test_rrqr(double* R, int ld, int n, int k, int rows, int* jpvt, double tol, double Tmax,
                               long long rrqr_iter, double* aux, int* niter, int* capped) {
-  return flam::rrqr_serial(R, ld, n, k, rows, jpvt, tol, Tmax, (int64_t)rrqr_iter, aux, niter, capped);
+  return flam::rrqr_serial(R, 1, ld, n, k, rows, jpvt, tol, Tmax, (int64_t)rrqr_iter, aux, niter, capped);
 }
