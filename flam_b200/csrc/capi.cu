@@ -764,7 +764,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       // shared by the compress and elimination kernels of this step
       const int n = (int)nslf[q];
       const bool tc = n <= kTcMaxN;
-      const bool c_glob = tc ? compress_tc_smem_bytes(n) > kTcSmemMax : n > kSmemN;
+      const bool c_glob = tc ? compress_tc_smem_bytes(n) > tc_smem_max() : n > kSmemN;
       const bool e_glob = n > kSmemN;
       t.scr_off = -1;
       elim_scr[q] = -1;

@@ -15,7 +15,9 @@
 // sqrt(eps) downdating threshold, min(m, n) steps), then rank, T = R11\R12 and
 // the RRQR refinement (rrqr.cuh) exactly as the per-column kernel in
 // compress.cu, whose results this kernel reproduces up to rounding.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -54,9 +56,8 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 // (thread g holds panel rows g*B .. g*B+B-1): annihilates the panel's column j
 // into R(j,j) (DLARFG conventions).
 template <int B, int G>
-__device__ __forceinline__ void reflect_col(double (&p)[B], double* R, int ld, int j, int g, unsigned gmask,
-                                            double* vb, double* tau_out) {
-  const double al = R[(int64_t)j * ld + j];
+__device__ __forceinline__ void reflect_col(double (&p)[B], double al, double* R, int ld, int j, int g,
+                                            unsigned gmask, double* vb, double* tau_out) {
   double sig = 0.0;
 #pragma unroll
   for (int i = 0; i < B; ++i) sig += p[i] * p[i];
@@ -216,11 +217,15 @@ __global__ void __launch_bounds__(B == 32 ? 512 : 1024) k_compress_tc(CompressAr
         }
       }
     }
-    // reflector 0 of this panel, formed by its owners
-    if (col == 0) reflect_col<B, G>(p, R, ld, 0, g, gmask, vbuf[0], &tau2[0]);
+    // reflector 0 of this panel, formed by its owners.  Thread col is the only
+    // writer of column col of R, so it reads R(j+1, col) one reflector ahead
+    // (the load overlaps step j and its barrier).
+    double rcur = col < n ? R[col] : 0.0;   // R(0, col)
+    if (col == 0) reflect_col<B, G>(p, rcur, R, ld, 0, g, gmask, vbuf[0], &tau2[0]);
     __syncthreads();
     for (int j = 0; j < n; ++j) {
       const int b = j & 1;
+      const double rnext = (col > j && col < n && j + 1 < n) ? R[(int64_t)(j + 1) * ld + col] : 0.0;
       const double tau = tau2[b];
       if (tau != 0.0 && col > j && col < n) {
         const double* v = vbuf[b] + g * B;
@@ -232,13 +237,14 @@ __global__ void __launch_bounds__(B == 32 ? 512 : 1024) k_compress_tc(CompressAr
           w2 += v[i + 2] * p[i + 2];
           w3 += v[i + 3] * p[i + 3];
         }
-        const double rjc = R[(int64_t)j * ld + col];
-        const double tw = tau * (rjc + group_sum<G>((w0 + w1) + (w2 + w3), gmask));
-        if (g == 0) R[(int64_t)j * ld + col] = rjc - tw;
+        const double tw = tau * (rcur + group_sum<G>((w0 + w1) + (w2 + w3), gmask));
+        if (g == 0) R[(int64_t)j * ld + col] = rcur - tw;
 #pragma unroll
         for (int i = 0; i < B; ++i) p[i] -= tw * v[i];
       }
-      if (col == j + 1 && col < n) reflect_col<B, G>(p, R, ld, j + 1, g, gmask, vbuf[b ^ 1], &tau2[b ^ 1]);
+      if (col == j + 1 && col < n)
+        reflect_col<B, G>(p, rnext, R, ld, j + 1, g, gmask, vbuf[b ^ 1], &tau2[b ^ 1]);
+      rcur = rnext;
       __syncthreads();
     }
   }
@@ -302,16 +308,34 @@ __global__ void __launch_bounds__(B == 32 ? 512 : 1024) k_compress_tc(CompressAr
     const double tau = tau2[0];
     if (c > i && c < n) {
       if (tau != 0.0) {
-        double w0 = R[(int64_t)i * ld + c], w1 = 0.0;
+        // loads in groups of four so several are in flight (R may live in L2)
+        double w0 = R[(int64_t)i * ld + c], w1 = 0.0, w2 = 0.0, w3 = 0.0;
         int r = i + 1;
-        for (; r + 1 < n; r += 2) {
-          w0 += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + c];
-          w1 += R[(int64_t)(r + 1) * ld + i] * R[(int64_t)(r + 1) * ld + c];
+        for (; r + 3 < n; r += 4) {
+          const double a0 = R[(int64_t)r * ld + i], a1 = R[(int64_t)(r + 1) * ld + i];
+          const double a2 = R[(int64_t)(r + 2) * ld + i], a3 = R[(int64_t)(r + 3) * ld + i];
+          const double b0 = R[(int64_t)r * ld + c], b1 = R[(int64_t)(r + 1) * ld + c];
+          const double b2 = R[(int64_t)(r + 2) * ld + c], b3 = R[(int64_t)(r + 3) * ld + c];
+          w0 += a0 * b0;
+          w1 += a1 * b1;
+          w2 += a2 * b2;
+          w3 += a3 * b3;
         }
-        if (r < n) w0 += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + c];
-        const double tw = tau * (w0 + w1);
+        for (; r < n; ++r) w0 += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + c];
+        const double tw = tau * ((w0 + w1) + (w2 + w3));
         R[(int64_t)i * ld + c] -= tw;
-        for (int rr = i + 1; rr < n; ++rr) R[(int64_t)rr * ld + c] -= tw * R[(int64_t)rr * ld + i];
+        int rr = i + 1;
+        for (; rr + 3 < n; rr += 4) {
+          const double a0 = R[(int64_t)rr * ld + i], a1 = R[(int64_t)(rr + 1) * ld + i];
+          const double a2 = R[(int64_t)(rr + 2) * ld + i], a3 = R[(int64_t)(rr + 3) * ld + i];
+          const double b0 = R[(int64_t)rr * ld + c], b1 = R[(int64_t)(rr + 1) * ld + c];
+          const double b2 = R[(int64_t)(rr + 2) * ld + c], b3 = R[(int64_t)(rr + 3) * ld + c];
+          R[(int64_t)rr * ld + c] = b0 - tw * a0;
+          R[(int64_t)(rr + 1) * ld + c] = b1 - tw * a1;
+          R[(int64_t)(rr + 2) * ld + c] = b2 - tw * a2;
+          R[(int64_t)(rr + 3) * ld + c] = b3 - tw * a3;
+        }
+        for (; rr < n; ++rr) R[(int64_t)rr * ld + c] -= tw * R[(int64_t)rr * ld + i];
       }
       if (vn1[c] != 0.0) {  // partial norm downdate (xLAQP2)
         double temp = fabs(R[(int64_t)i * ld + c]) / vn1[c];
@@ -423,6 +447,17 @@ void launch_b(const CompressArgs& a, int ntask, int nt, size_t smem, cudaStream_
 }
 
 }  // namespace
+
+size_t tc_smem_max() {
+  static size_t v = [] {
+    const char* e = std::getenv("FLAM_TC_SMEM_MAX");
+    // default: only the small boxes (n <~ 64) keep R in shared memory; larger ones
+    // read it from L2 with one-step prefetch, which leaves room for more CTAs per SM
+    const long long x = e ? std::atoll(e) : 40 * 1024;
+    return (size_t)std::min<long long>(std::max<long long>(x, 0), 200 * 1024);
+  }();
+  return v;
+}
 
 int64_t compress_tc_doubles(int n) { return (int64_t)n * (n | 1) + 8 * (int64_t)n + n / 2 + 2; }
 

@@ -30,7 +30,9 @@ void launch_compress(const CompressArgs& a, int ntask, size_t smem, cudaStream_t
 // (compress_tc_threads(n)), work arrays of compress_tc_doubles(n) in shared memory
 // when they fit kTcSmemMax, else in the task's global scratch.
 constexpr int kTcMaxN = 1024;
-constexpr size_t kTcSmemMax = 200 * 1024;
+// Work arrays above this many bytes go to global scratch (L2); tunable through
+// FLAM_TC_SMEM_MAX (bytes) to trade shared-memory residency for occupancy.
+size_t tc_smem_max();
 int64_t compress_tc_doubles(int n);
 size_t compress_tc_smem_bytes(int n);
 int compress_tc_threads(int n);
