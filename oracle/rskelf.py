@@ -332,3 +332,174 @@ def print_stats(F):
             s["lvl"], s["nblk"], s["nrem1"], s["nrem2"], s["nrem1"] / s["nblk"], s["nrem2"] / s["nblk"], s["time"]))
     lines.append("-" * 69)
     return "\n".join(lines)
+
+
+def _sv_half(F, X, trans, upward):
+    sol = sl.solve_triangular
+    symm = F["symm"]
+    fs = F["factors"] if upward else list(reversed(F["factors"]))
+    for f in fs:
+        sk, rd = f["sk"], f["rd"]
+        if upward:
+            X[rd] -= f["T"].T @ X[sk]
+            if symm in ("n", "s") and trans == "n":
+                X[rd] = sol(f["L"], X[rd[f["p"]]], lower=True, unit_diagonal=True)
+                X[sk] -= f["E"] @ X[rd]
+            elif symm in ("n", "s"):
+                X[rd] = sol(f["U"], X[rd], trans="T", lower=False)
+                X[sk] -= f["F"].T @ X[rd]
+            elif symm == "h":
+                X[rd] = sol(f["L"], X[rd], lower=True, unit_diagonal=True)
+                X[sk] -= f["E"] @ X[rd]
+                X[rd] = np.linalg.solve(f["U"], X[rd])
+            else:
+                X[rd] = sol(f["L"], X[rd], lower=True)
+                X[sk] -= f["E"] @ X[rd]
+        else:
+            if symm in ("n", "s") and trans == "n":
+                X[rd] -= f["F"] @ X[sk]
+                X[rd] = sol(f["U"], X[rd], lower=False)
+            elif symm in ("n", "s"):
+                X[rd] -= f["E"].T @ X[sk]
+                X[rd[f["p"]]] = sol(f["L"], X[rd], trans="T", lower=True, unit_diagonal=True)
+            elif symm == "h":
+                X[rd] -= f["E"].T @ X[sk]
+                X[rd] = sol(f["L"], X[rd], trans="T", lower=True, unit_diagonal=True)
+            else:
+                X[rd] -= f["E"].T @ X[sk]
+                X[rd] = sol(f["L"], X[rd], trans="T", lower=True)
+            X[sk] -= f["T"] @ X[rd]
+    return X
+
+
+def _mv_half(F, X, trans, upward):
+    symm = F["symm"]
+    fs = F["factors"] if upward else list(reversed(F["factors"]))
+    for f in fs:
+        sk, rd = f["sk"], f["rd"]
+        if upward:
+            X[sk] += f["T"] @ X[rd]
+            if symm in ("n", "s") and trans == "n":
+                X[rd] = f["U"] @ X[rd]
+                X[rd] += f["F"] @ X[sk]
+            elif symm in ("n", "s"):
+                X[rd] = f["L"].T @ X[rd[f["p"]]]
+                X[rd] += f["E"].T @ X[sk]
+            elif symm == "h":
+                X[rd] = f["L"].T @ X[rd]
+                X[rd] += f["E"].T @ X[sk]
+                X[rd] = f["U"] @ X[rd]
+            else:
+                X[rd] = f["L"].T @ X[rd]
+                X[rd] += f["E"].T @ X[sk]
+        else:
+            if symm in ("n", "s") and trans == "n":
+                X[sk] += f["E"] @ X[rd]
+                X[rd[f["p"]]] = f["L"] @ X[rd]
+            elif symm in ("n", "s"):
+                X[sk] += f["F"].T @ X[rd]
+                X[rd] = f["U"].T @ X[rd]
+            else:
+                X[sk] += f["E"] @ X[rd]
+                X[rd] = f["L"] @ X[rd]
+            X[rd] += f["T"].T @ X[sk]
+    return X
+
+
+def _prep(X):
+    X = np.array(X, dtype=np.float64, copy=True)
+    vec = X.ndim == 1
+    return (X[:, None] if vec else X), vec
+
+
+def rskelf_cholmv(F, X, trans="n"):
+    """Y = C X with F = C C' (symm 'p').  rskelf/rskelf_cholmv.m:15-50."""
+    if F["symm"] != "p":
+        raise ValueError("FLAM:rskelf_cholmv:invalidSymm: Symmetry parameter must be 'P'.")
+    trans = chktrans(trans)
+    X, vec = _prep(X)
+    Y = _mv_half(F, X, "n", upward=(trans != "n"))     # 'n': downward half; 'c'/'t': upward half
+    return Y[:, 0] if vec else Y
+
+
+def rskelf_cholsv(F, X, trans="n"):
+    """Y = C \\ X.  rskelf/rskelf_cholsv.m:15-50."""
+    if F["symm"] != "p":
+        raise ValueError("FLAM:rskelf_cholsv:invalidSymm: Symmetry parameter must be 'P'.")
+    trans = chktrans(trans)
+    X, vec = _prep(X)
+    Y = _sv_half(F, X, "n", upward=(trans == "n"))     # 'n': upward half; 'c'/'t': downward half
+    return Y[:, 0] if vec else Y
+
+
+def rskelf_logdet(F):
+    """log det of the factored matrix, imaginary part in [0, 2 pi).  rskelf/rskelf_logdet.m:11-33."""
+    ld = 0.0 + 0.0j
+    for f in F["factors"]:
+        if F["symm"] == "p":
+            ld += 2 * np.sum(np.log(np.diag(f["L"]).astype(complex)))
+        elif F["symm"] == "h":
+            ld += _logdet_ldl(f["U"])                                   # core/logdet_ldl.m
+        else:
+            ld += np.sum(np.log(np.diag(f["U"]).astype(complex))) + np.log(complex(_detperm(f["p"])))
+    return complex(ld.real, math.fmod(ld.imag, 2 * math.pi) % (2 * math.pi))
+
+
+def _detperm(p):
+    """Sign of a permutation (compat/detperm.m)."""
+    p = np.asarray(p)
+    seen = np.zeros(len(p), dtype=bool)
+    sgn = 1
+    for i in range(len(p)):
+        if not seen[i]:
+            j, L = i, 0
+            while not seen[j]:
+                seen[j] = True
+                j = p[j]
+                L += 1
+            if L % 2 == 0:
+                sgn = -sgn
+    return sgn
+
+
+def _logdet_ldl(D):
+    """core/logdet_ldl.m:6-12: 1x1 and 2x2 diagonal blocks of D."""
+    D = np.asarray(D)
+    one = np.count_nonzero(D, axis=0) == 1
+    ld = np.sum(np.log(np.diag(D)[one].astype(complex)))
+    idx = np.flatnonzero(~one)
+    for i in range(0, len(idx), 2):
+        b = D[np.ix_(idx[i:i + 2], idx[i:i + 2])]
+        ld += np.log(complex(np.linalg.det(b)))
+    return ld
+
+
+def rskelf_partial_info(F):
+    """[sk, S] = rskelf_partial_info(F).  rskelf/rskelf_partial_info.m."""
+    if "Si" in F:
+        return F["Si"], F["S"]
+    return np.zeros(0, np.int64), np.zeros((0, 0))
+
+
+def rskelf_partial_sv(F, X, svfun, trans="n"):
+    """Upward sweep, svfun on X(Si), downward sweep.  rskelf/rskelf_partial_sv.m:23-62."""
+    trans = chktrans(trans)
+    X, vec = _prep(X)
+    t = "n" if trans == "n" else "c"
+    X = _sv_half(F, X, t, True)
+    if "Si" in F and len(F["Si"]):
+        X[F["Si"]] = svfun(X[F["Si"]], t)
+    X = _sv_half(F, X, t, False)
+    return X[:, 0] if vec else X
+
+
+def rskelf_partial_mv(F, X, mvfun, trans="n"):
+    """Upward sweep, mvfun on X(Si), downward sweep.  rskelf/rskelf_partial_mv.m."""
+    trans = chktrans(trans)
+    X, vec = _prep(X)
+    t = "n" if trans == "n" else "c"
+    X = _mv_half(F, X, t, True)
+    if "Si" in F and len(F["Si"]):
+        X[F["Si"]] = mvfun(X[F["Si"]], t)
+    X = _mv_half(F, X, t, False)
+    return X[:, 0] if vec else X
