@@ -22,7 +22,12 @@ EXPORTS = (
     "flam_opts_default", "flam_hypoct", "flam_id", "flam_id_noalloc", "flam_rskelf", "flam_rskelf_batched", "flam_rskelf_sv", "flam_rskelf_mv",
     "flam_factor_info", "flam_tree_export", "flam_tree_perm", "flam_factor_sizes", "flam_factor_export",
     "flam_level_stats", "flam_factor_free", "flam_workspace_release", "flam_profile", "flam_last_error", "flam_version",
+    "flam_rskelf_cholmv", "flam_rskelf_cholsv", "flam_rskelf_logdet", "flam_partial_sizes", "flam_partial_export",
+    "flam_rskelf_partial_sv", "flam_rskelf_partial_mv",
 )
+
+# int fn(double* Y, int64_t n, int64_t nrhs, char trans, void* stream, void* ctx)
+SKEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_char, C.c_void_p, C.c_void_p)
 
 
 class FlamKernel(C.Structure):
@@ -93,9 +98,18 @@ def lib():
     L.flam_rskelf_batched.argtypes = [C.c_int, P, C.c_int, i64p, C.POINTER(FlamKernel), C.c_double, C.c_double,
                                       C.POINTER(FlamProxy), C.POINTER(FlamOpts), C.POINTER(P)]
     L.flam_rskelf_batched.restype = C.c_int
-    for f in ("flam_rskelf_sv", "flam_rskelf_mv"):
+    for f in ("flam_rskelf_sv", "flam_rskelf_mv", "flam_rskelf_cholmv", "flam_rskelf_cholsv"):
         getattr(L, f).argtypes = [P, P, C.c_int64, C.c_int64, C.c_char]
         getattr(L, f).restype = C.c_int
+    for f in ("flam_rskelf_partial_sv", "flam_rskelf_partial_mv"):
+        getattr(L, f).argtypes = [P, P, C.c_int64, C.c_int64, C.c_char, SKEL_FN, P]
+        getattr(L, f).restype = C.c_int
+    L.flam_rskelf_logdet.argtypes = [P, dp, dp]
+    L.flam_rskelf_logdet.restype = C.c_int
+    L.flam_partial_sizes.argtypes = [P, C.c_int, i64p, i64p]
+    L.flam_partial_sizes.restype = C.c_int
+    L.flam_partial_export.argtypes = [P, C.c_int, i64p, i64p, i64p, dp]
+    L.flam_partial_export.restype = C.c_int
     L.flam_factor_info.argtypes = [P, C.POINTER(FlamInfo)]
     L.flam_factor_info.restype = C.c_int
     L.flam_tree_export.argtypes = [P, C.c_int, C.POINTER(C.c_int), i64p, i64p, i64p, i64p, i64p, dp, dp, i64p,

@@ -3,6 +3,12 @@
     F = rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None)     rskelf/rskelf.m:109
     Y = rskelf_sv(F, X, trans='n')                                  rskelf/rskelf_sv.m:13
     Y = rskelf_mv(F, X, trans='n')                                  rskelf/rskelf_mv.m:13
+    Y = rskelf_cholmv(F, X, trans='n')                              rskelf/rskelf_cholmv.m:15
+    Y = rskelf_cholsv(F, X, trans='n')                              rskelf/rskelf_cholsv.m:15
+    ld = rskelf_logdet(F)                                           rskelf/rskelf_logdet.m:11
+    Si, S = rskelf_partial_info(F)                                  rskelf/rskelf_partial_info.m:12
+    Y = rskelf_partial_sv(F, X, svfun, trans='n')                   rskelf/rskelf_partial_sv.m:23
+    Y = rskelf_partial_mv(F, X, mvfun, trans='n')                   rskelf/rskelf_partial_mv.m:23
     T = hypoct(x, occ, lvlmax=inf, ext=None)                        core/hypoct.m:51
     P = hypoct_perm(T)                                              core/hypoct_perm.m:11
 
@@ -195,9 +201,9 @@ class Factor:
     def mv_(self, X, trans="n"):
         return self._apply(X, trans, False)
 
-    def _apply(self, X, trans, solve):
+    def _apply(self, X, trans, solve, name=None, extra=()):
         L = _lib.lib()
-        fn = L.flam_rskelf_sv if solve else L.flam_rskelf_mv
+        fn = getattr(L, name) if name else (L.flam_rskelf_sv if solve else L.flam_rskelf_mv)
         if _is_cuda_tensor(X):
             import torch
             if X.dtype != torch.float64:
@@ -208,13 +214,63 @@ class Factor:
                 if X.stride(0) != 1:
                     raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: X must be column-major (X.t().contiguous().t())")
                 ptr, ld, nrhs = X.data_ptr(), X.stride(1), X.shape[1]
-            _lib.check(fn(self._h, C.c_void_p(ptr), ld, nrhs, str(trans).encode()[:1]))
+            _lib.check(fn(self._h, C.c_void_p(ptr), ld, nrhs, str(trans).encode()[:1], *extra))
             return X
         if not (isinstance(X, np.ndarray) and X.dtype == np.float64 and (X.ndim == 1 or X.flags.f_contiguous)):
             raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: X must be a float64 Fortran-ordered array")
         nrhs = 1 if X.ndim == 1 else X.shape[1]
-        _lib.check(fn(self._h, C.c_void_p(X.ctypes.data), X.shape[0], nrhs, str(trans).encode()[:1]))
+        _lib.check(fn(self._h, C.c_void_p(X.ctypes.data), X.shape[0], nrhs, str(trans).encode()[:1], *extra))
         return X
+
+    # ------------------------------------------------------- partial factorization
+    def partial_info(self, inst=0):
+        """[Si, S] = rskelf_partial_info(F): remaining skeletons (0-based, ascending) and the
+        sparse update S, so that A(Si,Si) + S is the skeleton system left to the caller."""
+        import scipy.sparse as sp
+        L = _lib.lib()
+        i64 = C.c_int64
+        Sn, nnz = i64(), i64()
+        _lib.check(L.flam_partial_sizes(self._h, inst, C.byref(Sn), C.byref(nnz)))
+        n, z = Sn.value, nnz.value
+        Si = np.zeros(max(n, 1), np.int64)
+        cp = np.zeros(n + 1, np.int64)
+        ri = np.zeros(max(z, 1), np.int64)
+        v = np.zeros(max(z, 1))
+        p64 = lambda a: a.ctypes.data_as(C.POINTER(i64))  # noqa: E731
+        _lib.check(L.flam_partial_export(self._h, inst, p64(Si), p64(cp), p64(ri),
+                                         v.ctypes.data_as(C.POINTER(C.c_double))))
+        return Si[:n], sp.csc_matrix((v[:z], ri[:z], cp), shape=(n, n))
+
+    def _partial(self, X, fun, trans, solve):
+        host = not _is_cuda_tensor(X)
+        err = []
+
+        def cb(yptr, n, nrhs, tr, stream, ctx):
+            try:
+                import torch
+                torch.cuda.synchronize()
+                Y = torch.as_tensor(_DevBlock(yptr, n, nrhs), device="cuda")
+                arg = Y.cpu().numpy().copy(order="F") if host else Y.clone()
+                out = fun(arg, tr.decode())
+                if tuple(np.shape(out)) != (n, nrhs) and not (nrhs == 1 and np.size(out) == n):
+                    raise ValueError(f"skeleton function returned shape {np.shape(out)}, expected {(n, nrhs)}")
+                Y.copy_(torch.as_tensor(np.asarray(out) if host else out, dtype=torch.float64).reshape(n, nrhs))
+                torch.cuda.synchronize()
+                return 0
+            except Exception as e:  # noqa: BLE001 - re-raised after the call returns
+                err.append(e)
+                return 1
+
+        cfn = _lib.SKEL_FN(cb)
+        name = "flam_rskelf_partial_sv" if solve else "flam_rskelf_partial_mv"
+        try:
+            self._apply(X, trans, solve, name, (cfn, None))
+        except _lib.FlamError:
+            if err:
+                raise err[0]
+            raise
+        return X
+
 
 
 def _check_handles(A, pxyfun):
@@ -288,6 +344,55 @@ def rskelf_sv(F, X, trans="n"):
 def rskelf_mv(F, X, trans="n"):
     """Y = rskelf_mv(F, X, trans): returns a new array."""
     return F.mv_(_fresh_copy(X), trans)
+
+
+def rskelf_cholmv(F, X, trans="n"):
+    """Y = C X (C' X for 't'/'c') with F = C C' (symm 'p').   rskelf/rskelf_cholmv.m:15-50."""
+    return F._apply(_fresh_copy(X), trans, False, "flam_rskelf_cholmv")
+
+
+def rskelf_cholsv(F, X, trans="n"):
+    """Y = C \\ X (C' \\ X for 't'/'c') with F = C C' (symm 'p').   rskelf/rskelf_cholsv.m:15-50."""
+    return F._apply(_fresh_copy(X), trans, True, "flam_rskelf_cholsv")
+
+
+def rskelf_logdet(F):
+    """log det of the factored matrix, imaginary part in [0, 2 pi).   rskelf/rskelf_logdet.m:11-33.
+
+    A batched handle returns one value per instance."""
+    n = F.ninst
+    re = np.zeros(n)
+    im = np.zeros(n)
+    _lib.check(_lib.lib().flam_rskelf_logdet(F.handle, re.ctypes.data_as(C.POINTER(C.c_double)),
+                                             im.ctypes.data_as(C.POINTER(C.c_double))))
+    out = [complex(a, b) for a, b in zip(re, im)]
+    return out[0] if n == 1 else out
+
+
+def rskelf_partial_info(F, inst=0):
+    """[Si, S] = rskelf_partial_info(F)   rskelf/rskelf_partial_info.m:12-20 (S: scipy CSC)."""
+    return F.partial_info(inst)
+
+
+def rskelf_partial_sv(F, X, svfun, trans="n"):
+    """Upward sweep, X(Si,:) = svfun(X(Si,:), trans), downward sweep.   rskelf/rskelf_partial_sv.m:23-62.
+
+    svfun gets a NumPy array for a NumPy X and a CUDA tensor for a CUDA X; trans is 'n' or 'c'.
+    With several instances X(Si,:) stacks every instance's Si in instance order."""
+    return F._partial(_fresh_copy(X), svfun, trans, True)
+
+
+def rskelf_partial_mv(F, X, mvfun, trans="n"):
+    """Upward sweep, X(Si,:) = mvfun(X(Si,:), trans), downward sweep.   rskelf/rskelf_partial_mv.m:23-62."""
+    return F._partial(_fresh_copy(X), mvfun, trans, False)
+
+
+class _DevBlock:
+    """A column-major n x nrhs float64 block of device memory, seen through __cuda_array_interface__."""
+
+    def __init__(self, ptr, n, nrhs):
+        self.__cuda_array_interface__ = {"shape": (n, nrhs), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 2, "strides": (8, 8 * n)}
 
 
 def hypoct(x, occ, lvlmax=math.inf, ext=None):

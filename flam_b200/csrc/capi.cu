@@ -125,6 +125,13 @@ struct HostFac {
   int64_t fac_off, piv_off;
 };
 
+// An M block left when an instance stops: rows/columns ipool[idx_off, idx_off + n),
+// values (column-major n x n) at val_off of the host copy.
+struct KeptBlock {
+  int inst;
+  int64_t idx_off, n, val_off;
+};
+
 struct StepDev {
   DBuf<FacDesc> fac;
   int nfac = 0, kmax = 0, rmax = 0;
@@ -213,6 +220,12 @@ struct flam_factor {
   std::vector<std::vector<int64_t>> inst_lvp;     // per instance F.lvp
   std::vector<std::vector<LevelStat>> stats;
   std::vector<int64_t> rem;  // remaining points per instance
+  // partial factorization (rskelf.m:278-308): per instance the remaining skeletons Si
+  // (instance-local, ascending) and S in compressed-column form
+  std::vector<std::vector<int64_t>> Si, Scp, Sri;
+  std::vector<std::vector<double>> Sv;
+  DBuf<int64_t> Si_dev;      // global ids of every instance's Si, instance order
+  int64_t Sn_tot = 0;
   double t_tree = 0, t_factor = 0;
   int64_t warn = 0;
   bool profile = false;
@@ -243,6 +256,7 @@ struct flam_factor {
     ipool.release(st);
     fpool.release(st);
     ppool.release(st);
+    Si_dev.release(st);
     for (auto& q : steps) q.fac.release(st);
     cudaStreamSynchronize(st);
   }
@@ -595,6 +609,80 @@ void build_tree(flam_factor& F, double occ, const flam_opts& o) {
 }
 
 // --------------------------------------------------------------- factorization (K3-K7)
+// Remaining skeletons and their sparse system after a partial factorization
+// (rskelf.m:278-308): Si = the points of each instance that no factor eliminated,
+// S = the kept M blocks scattered to Si positions, in compressed-column form with
+// rows ascending (what MATLAB's sparse(I,J,V,Sn,Sn) holds; exact zeros dropped).
+void assemble_partial(flam_factor& F, const std::vector<KeptBlock>& kept, const std::vector<double>& val) {
+  const int ninst = F.ninst;
+  F.Si.assign(ninst, {});
+  F.Scp.assign(ninst, {0});
+  F.Sri.assign(ninst, {});
+  F.Sv.assign(ninst, {});
+  F.Sn_tot = 0;
+  int64_t nrem = 0;
+  for (auto v : F.rem) nrem += v;
+  if (nrem == 0) return;
+  const cudaStream_t s = F.s;
+  auto ids = download(F.ipool.p, F.ipool.n, s);
+  std::vector<uint8_t> gone((size_t)F.Ntot, 0);
+  for (const HostFac& h : F.hfac)
+    for (int64_t j = h.sk_off + h.k; j < h.sk_off + h.k + h.r; ++j) gone[ids[j]] = 1;
+  std::vector<int64_t> pos((size_t)F.Ntot, -1), glob;
+  for (int i = 0; i < ninst; ++i) {
+    for (int64_t g = F.inst_off[i]; g < F.inst_off[i + 1]; ++g)
+      if (!gone[g]) {
+        pos[g] = (int64_t)F.Si[i].size();
+        F.Si[i].push_back(g - F.inst_off[i]);
+        glob.push_back(g);
+      }
+    if ((int64_t)F.Si[i].size() != F.rem[i])
+      fail(FLAM_ERR_CUDA, "FLAM:gpu:internal: remaining point count disagrees with the factors");
+  }
+  F.Sn_tot = (int64_t)glob.size();
+  F.Si_dev.upload(glob, s);
+  // columns: each remaining point lies in at most one kept block
+  std::vector<std::vector<int64_t>> cnt(ninst);
+  for (int i = 0; i < ninst; ++i) cnt[i].assign(F.Si[i].size() + 1, 0);
+  struct Col { int64_t blk, a; };
+  std::vector<std::vector<Col>> owner(ninst);
+  for (int i = 0; i < ninst; ++i) owner[i].assign(F.Si[i].size(), Col{-1, -1});
+  std::vector<std::vector<int64_t>> order(kept.size());
+  for (size_t q = 0; q < kept.size(); ++q) {
+    const KeptBlock& kb = kept[q];
+    std::vector<int64_t> ps(kb.n);
+    for (int64_t a = 0; a < kb.n; ++a) {
+      ps[a] = pos[ids[kb.idx_off + a]];
+      if (ps[a] < 0) fail(FLAM_ERR_CUDA, "FLAM:gpu:internal: a kept skeleton was eliminated");
+      owner[kb.inst][ps[a]] = Col{(int64_t)q, a};
+    }
+    auto& ord = order[q];
+    ord.resize(kb.n);
+    for (int64_t a = 0; a < kb.n; ++a) ord[a] = a;
+    std::sort(ord.begin(), ord.end(), [&](int64_t x, int64_t y) { return ps[x] < ps[y]; });
+  }
+  for (int i = 0; i < ninst; ++i) {
+    const int64_t Sn = (int64_t)F.Si[i].size();
+    auto& cp = F.Scp[i];
+    auto& ri = F.Sri[i];
+    auto& v = F.Sv[i];
+    cp.assign(Sn + 1, 0);
+    for (int64_t c = 0; c < Sn; ++c) {
+      const Col o = owner[i][c];
+      if (o.blk >= 0) {
+        const KeptBlock& kb = kept[o.blk];
+        const double* M = val.data() + kb.val_off + o.a * kb.n;   // column a of the block
+        for (int64_t e : order[o.blk]) {
+          if (M[e] == 0.0) continue;
+          ri.push_back(pos[ids[kb.idx_off + e]]);
+          v.push_back(M[e]);
+        }
+      }
+      cp[c + 1] = (int64_t)ri.size();
+    }
+  }
+}
+
 void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   cudaStream_t s = F.s;
   const int ninst = F.ninst;
@@ -668,6 +756,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   // after the last step so that profiling adds no synchronisation
   std::vector<cudaEvent_t> step_ev;
   cudaEvent_t* pe = nullptr;
+  // M blocks still unfactored when an instance stops: (instance, ipool offset, n, offset in kept_val)
+  std::vector<KeptBlock> kept;
+  std::vector<double> kept_val;
+  const int64_t nrun = std::min<int64_t>(stop, maxsteps);
 
   for (int step = 0; step < maxsteps && step < stop; ++step) {
     // ---- boxes of this step: level nlvl_i - step of each instance
@@ -969,6 +1061,27 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       xlen[b] = (n - k > 0) ? k : n;
       Moff[b] = et[q].M_out;
     }
+    // the boxes of an instance's last processed level keep their M blocks: the
+    // remaining skeleton system of a partial factorization (rskelf.m:280-308)
+    {
+      const bool last = step + 1 == nrun;
+      std::vector<double> mh;
+      if (last && mtop > 0) mh = download(mpool[cur].p, mtop, s);
+      for (int q = 0; q < nb; ++q) {
+        const int32_t b = boxes[q];
+        const int i = F.binst[b];
+        if (!(last || F.nlvl[i] - step == 1) || xlen[b] == 0) continue;
+        const int64_t nn = xlen[b] * xlen[b];
+        kept.push_back(KeptBlock{i, xoff[b], xlen[b], (int64_t)kept_val.size()});
+        kept_val.resize(kept_val.size() + nn);
+        if (last) {
+          std::copy(mh.begin() + Moff[b], mh.begin() + Moff[b] + nn, kept_val.end() - nn);
+        } else {
+          auto v = download(mpool[cur].p + Moff[b], nn, s);
+          std::copy(v.begin(), v.end(), kept_val.end() - nn);
+        }
+      }
+    }
     // per instance: F.lvp and the verbose table row
     std::vector<int> seen(ninst, 0);
     for (int q = 0; q < nb; ++q) seen[F.binst[boxes[q]]] = 1;
@@ -1003,6 +1116,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   if (st & ST_NOT_SPD)
     fail(FLAM_ERR_NOT_SPD, "FLAM:rskelf:notPosDef: a redundant block is not positive definite (chol failed)");
   if (st & ST_SINGULAR) F.warn |= 2;
+  assemble_partial(F, kept, kept_val);
 }
 
 void print_table(const flam_factor& F) {
@@ -1153,7 +1267,16 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
   return FLAM_OK;
 }
 
-flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans, bool solve) {
+// Which halves of the sweeps an apply runs.
+enum : int { kUp = 1, kDown = 2, kBoth = 3 };
+
+// The sweeps of rskelf_sv / rskelf_mv (solve = true / false) on X, in place.
+// halves selects the upward and/or downward half; with a skeleton function fn
+// (partial factorization) X(Si,:) is passed to fn between the halves
+// (rskelf_partial_sv.m:33-62).  sweep_trans overrides trans for the sweeps
+// (the Cholesky halves always run the 'n' variant: rskelf_cholsv.m:32-50).
+flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans, bool solve,
+                  int halves = kBoth, flam_skel_fn fn = nullptr, void* ctx = nullptr, char sweep_trans = 0) {
   if (!F) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: NULL factor");
   trans = chktrans(trans);
   if (nrhs < 0 || ldx < F->Ntot) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: bad X dimensions");
@@ -1169,14 +1292,26 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   };
   auto hstart = std::chrono::steady_clock::now();
   mark(0);
-  const int t = trans == 'n' ? 0 : 1;   // real data: 't' == 'c' (rskelf_sv.m:22)
+  const char tc = trans == 'n' ? 'n' : 'c';   // real data: 't' == 'c' (rskelf_sv.m:22)
+  const int t = (sweep_trans ? sweep_trans : tc) == 'n' ? 0 : 1;
   const int64_t N = F->Ntot;
   const bool dev = is_device_ptr(X);
   double* Xd = X;
   int64_t ld = ldx;
   Workspace& ws = workspace(F->dev, s);
-  auto& tmp = ws.tmp;
-  auto& W = ws.W;
+  // with a skeleton function the work arrays are private to this call: the
+  // function may itself apply another factorization on the same stream
+  const bool own = fn && F->Sn_tot > 0;
+  DBuf<double> own_tmp, own_W, own_Y;
+  struct Release {
+    DBuf<double>* b[3];
+    cudaStream_t s;
+    ~Release() {
+      for (auto* q : b) q->release(s);
+    }
+  } release_own{{&own_tmp, &own_W, &own_Y}, s};
+  auto& tmp = own ? own_tmp : ws.tmp;
+  auto& W = own ? own_W : ws.W;
   if (!dev) {
     tmp.ensure(N * nrhs, s);
     CK(cudaMemcpy2DAsync(tmp.p, sizeof(double) * N, X, sizeof(double) * ldx, sizeof(double) * N, nrhs,
@@ -1217,10 +1352,32 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
     F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)nrhs;
   };
   F->prof.launches += 2;  // layout changes
-  a.op = solve ? 0 : 2;
-  for (int q = 0; q < ns; ++q) sweep(q);
-  a.op = solve ? 1 : 3;
-  for (int q = ns - 1; q >= 0; --q) sweep(q);
+  if (halves & kUp) {
+    a.op = solve ? 0 : 2;
+    for (int q = 0; q < ns; ++q) sweep(q);
+  }
+  if (fn && F->Sn_tot > 0) {
+    // X(Si,:) = fn(X(Si,:), trans) on a column-major copy
+    const int64_t Sn = F->Sn_tot;
+    auto& Y = own_Y;
+    Y.ensure(Sn * nrhs, s);
+    launch_rows_pm(W.p, (int)nrhs, F->Si_dev.p, Sn, Y.p, 0, s);
+    CK(cudaGetLastError());
+    const int rc = fn(Y.p, Sn, nrhs, tc, (void*)s, ctx);
+    if (rc != 0 && F->profile) {
+      cudaEventDestroy(F->pend[0]);
+      cudaEventDestroy(F->pend[1]);
+    }
+    if (rc != 0)
+      fail(FLAM_ERR_ARG, "%s:callback: the skeleton function returned %d",
+           solve ? "FLAM:rskelf_partial_sv" : "FLAM:rskelf_partial_mv", rc);
+    launch_rows_pm(W.p, (int)nrhs, F->Si_dev.p, Sn, Y.p, 1, s);
+    F->prof.launches += 2;
+  }
+  if (halves & kDown) {
+    a.op = solve ? 1 : 3;
+    for (int q = ns - 1; q >= 0; --q) sweep(q);
+  }
   if (F->profile) {
     CK(cudaEventRecord(F->pend[1], s));
     F->has_pend = true;
@@ -1424,6 +1581,100 @@ flam_status flam_rskelf_sv(const flam_factor* F, double* X, int64_t ldx, int64_t
 
 flam_status flam_rskelf_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {
   return guard([&] { return apply(F, X, ldx, nrhs, trans, false); });
+}
+
+flam_status flam_rskelf_cholmv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {
+  return guard([&] {
+    if (F && F->symm != 'p') fail(FLAM_ERR_ARG, "FLAM:rskelf_cholmv:invalidSymm: Symmetry parameter must be 'P'.");
+    const char t = F ? chktrans(trans) : 'n';
+    return apply(F, X, ldx, nrhs, trans, false, t == 'n' ? kDown : kUp, nullptr, nullptr, 'n');
+  });
+}
+
+flam_status flam_rskelf_cholsv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {
+  return guard([&] {
+    if (F && F->symm != 'p') fail(FLAM_ERR_ARG, "FLAM:rskelf_cholsv:invalidSymm: Symmetry parameter must be 'P'.");
+    const char t = F ? chktrans(trans) : 'n';
+    return apply(F, X, ldx, nrhs, trans, true, t == 'n' ? kUp : kDown, nullptr, nullptr, 'n');
+  });
+}
+
+flam_status flam_rskelf_partial_sv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans,
+                                   flam_skel_fn fn, void* ctx) {
+  return guard([&] {
+    if (!fn) fail(FLAM_ERR_ARG, "FLAM:rskelf_partial_sv:invalidArg: svfun is NULL");
+    return apply(F, X, ldx, nrhs, trans, true, kBoth, fn, ctx);
+  });
+}
+
+flam_status flam_rskelf_partial_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans,
+                                   flam_skel_fn fn, void* ctx) {
+  return guard([&] {
+    if (!fn) fail(FLAM_ERR_ARG, "FLAM:rskelf_partial_mv:invalidArg: mvfun is NULL");
+    return apply(F, X, ldx, nrhs, trans, false, kBoth, fn, ctx);
+  });
+}
+
+flam_status flam_rskelf_logdet(const flam_factor* F, double* re, double* im) {
+  return guard([&] {
+    if (!F) fail(FLAM_ERR_ARG, "FLAM:rskelf_logdet:invalidArg: NULL factor");
+    if (F->symm == 'h') fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h' is not built on the device");
+    const cudaStream_t s = F->s;
+    const int64_t nf = (int64_t)F->hfac.size();
+    std::vector<double> sr(F->ninst, 0.0);
+    std::vector<int64_t> par(F->ninst, 0);
+    if (nf > 0) {
+      DBuf<double> out;
+      out.resize(2 * nf, s);
+      int64_t base = 0;
+      for (const StepDev& sd : F->steps) {
+        launch_logdet(sd.fac.p, sd.nfac, F->fpool.p, F->ppool.p, F->symm == 'p', out.p + 2 * base, s);
+        F->prof.launches += sd.nfac > 0;
+        base += sd.nfac;
+      }
+      CK(cudaGetLastError());
+      auto h = download(out.p, 2 * nf, s);
+      out.release(s);
+      // per instance, in factor order (rskelf_logdet.m:18-29)
+      for (int i = 0; i < F->ninst; ++i)
+        for (int64_t f : F->inst_fac[i]) {
+          sr[i] += h[2 * f];
+          par[i] += (int64_t)h[2 * f + 1];
+        }
+    }
+    const double pi = 3.14159265358979323846;
+    for (int i = 0; i < F->ninst; ++i) {
+      if (re) re[i] = sr[i];
+      if (im) im[i] = (par[i] & 1) ? pi : 0.0;   // mod(imag, 2*pi) of a multiple of pi
+    }
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_partial_sizes(const flam_factor* F, int inst, int64_t* Sn, int64_t* nnz) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst) fail(FLAM_ERR_ARG, "FLAM:rskelf_partial_info:invalidArg: bad instance");
+    const bool have = (int)F->Si.size() == F->ninst;
+    if (Sn) *Sn = have ? (int64_t)F->Si[inst].size() : 0;
+    if (nnz) *nnz = have ? (int64_t)F->Sri[inst].size() : 0;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_partial_export(const flam_factor* F, int inst, int64_t* Si, int64_t* colptr, int64_t* rowind,
+                                double* val) {
+  return guard([&] {
+    if (!F || inst < 0 || inst >= F->ninst) fail(FLAM_ERR_ARG, "FLAM:rskelf_partial_info:invalidArg: bad instance");
+    if ((int)F->Si.size() != F->ninst) {
+      if (colptr) colptr[0] = 0;
+      return FLAM_OK;
+    }
+    if (Si) std::copy(F->Si[inst].begin(), F->Si[inst].end(), Si);
+    if (colptr) std::copy(F->Scp[inst].begin(), F->Scp[inst].end(), colptr);
+    if (rowind) std::copy(F->Sri[inst].begin(), F->Sri[inst].end(), rowind);
+    if (val) std::copy(F->Sv[inst].begin(), F->Sv[inst].end(), val);
+    return FLAM_OK;
+  });
 }
 
 flam_status flam_factor_info(const flam_factor* F, flam_info* info) {

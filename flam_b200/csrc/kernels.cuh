@@ -84,5 +84,12 @@ void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t
 // Layout changes for the user's column-major X (N x nrhs, ld) <-> point-major work array.
 void launch_to_pointmajor(const double* X, int64_t ld, int64_t N, int nrhs, double* W, cudaStream_t s);
 void launch_from_pointmajor(const double* W, int64_t N, int nrhs, double* X, int64_t ld, cudaStream_t s);
+// Rows idx (n of them) of the point-major W <-> column-major n x nrhs Y; dir 0 gathers, 1 scatters.
+void launch_rows_pm(double* W, int nrhs, const int64_t* idx, int64_t n, double* Y, int dir, cudaStream_t s);
+
+// Per-factor log-determinant terms of one step: out[2f] = sum log|diag| (x2 if chol),
+// out[2f+1] = parity of (negative diagonal entries + inversions of p).
+void launch_logdet(const FacDesc* fac, int nfac, const double* fpool, const int32_t* ppool, int chol, double* out,
+                   cudaStream_t s);
 
 }  // namespace flam

@@ -288,7 +288,46 @@ __global__ void k_from_pm(const double* W, int64_t N, int nrhs, double* X, int64
   }
 }
 
+// Rows idx of the point-major work array <-> a column-major n x nrhs block Y
+// (X(Si,:) of a partial factorization).  dir 0: gather into Y; 1: scatter back.
+__global__ void k_rows_pm(double* W, int nrhs, const int64_t* idx, int64_t n, double* Y, int dir) {
+  __shared__ double tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32;
+  if (dir == 0) {
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t i = i0 + q;
+      const int c = c0 + threadIdx.x;
+      tile[q][threadIdx.x] = (i < n && c < nrhs) ? W[idx[i] * nrhs + c] : 0.0;
+    }
+    __syncthreads();
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t i = i0 + threadIdx.x;
+      const int c = c0 + q;
+      if (i < n && c < nrhs) Y[i + (int64_t)c * n] = tile[threadIdx.x][q];
+    }
+  } else {
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t i = i0 + threadIdx.x;
+      const int c = c0 + q;
+      tile[q][threadIdx.x] = (i < n && c < nrhs) ? Y[i + (int64_t)c * n] : 0.0;
+    }
+    __syncthreads();
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+      const int64_t i = i0 + q;
+      const int c = c0 + threadIdx.x;
+      if (i < n && c < nrhs) W[idx[i] * nrhs + c] = tile[threadIdx.x][q];
+    }
+  }
+}
+
 }  // namespace
+
+void launch_rows_pm(double* W, int nrhs, const int64_t* idx, int64_t n, double* Y, int dir, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return;
+  dim3 g((unsigned)((n + 31) / 32), (nrhs + 31) / 32);
+  k_rows_pm<<<g, dim3(32, 8), 0, s>>>(W, nrhs, idx, n, Y, dir);
+}
 
 void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t s) {
   if (nfac <= 0 || a.nrhs <= 0) return;

@@ -164,6 +164,47 @@ FLAM_API flam_status flam_rskelf_sv(const flam_factor* F, double* X, int64_t ldx
 /* Y = rskelf_mv(F, X, trans), in place.  rskelf/rskelf_mv.m:13-36. */
 FLAM_API flam_status flam_rskelf_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans);
 
+/* Y = rskelf_cholmv(F, X, trans): Y = C X ('n') or C' X ('t'/'c') for F = C C', in place.
+ * One half of the 'p' multiply: the downward half for 'n', the upward half otherwise.
+ * rskelf/rskelf_cholmv.m:15-50.  F must have symm 'p' (FLAM:rskelf_cholmv:invalidSymm). */
+FLAM_API flam_status flam_rskelf_cholmv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans);
+
+/* Y = rskelf_cholsv(F, X, trans): Y = C \ X ('n') or C' \ X, in place.  The upward half of
+ * the 'p' solve for 'n', the downward half otherwise.  rskelf/rskelf_cholsv.m:15-50. */
+FLAM_API flam_status flam_rskelf_cholsv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans);
+
+/* ld = rskelf_logdet(F): log det of the factored matrix, one complex number per instance
+ * (re[i] + 1i*im[i], im in [0, 2 pi)).  rskelf/rskelf_logdet.m:11-33: 2 sum log diag(L)
+ * for 'p'; sum log diag(U) + log detperm(p) for 'n'/'s'.  Either pointer may be NULL. */
+FLAM_API flam_status flam_rskelf_logdet(const flam_factor* F, double* re, double* im);
+
+/* The remaining skeleton system of a partial factorization (opts.stop), per instance:
+ * [Si, S] = rskelf_partial_info(F) -- rskelf/rskelf_partial_info.m:12-20, assembled as in
+ * rskelf/rskelf.m:278-308.  The skeleton block left to the caller is A(Si,Si) + S.
+ * flam_partial_sizes gives Sn = numel(Si) and nnz(S); flam_partial_export fills Si (Sn,
+ * 0-based, ascending, instance-local) and S in compressed-column form (colptr: Sn+1, rowind
+ * and val: nnz; rows ascending in each column, exact zeros dropped like MATLAB's sparse).
+ * A complete factorization has Sn = 0.  Any output pointer may be NULL. */
+FLAM_API flam_status flam_partial_sizes(const flam_factor* F, int inst, int64_t* Sn, int64_t* nnz);
+FLAM_API flam_status flam_partial_export(const flam_factor* F, int inst, int64_t* Si, int64_t* colptr,
+                                         int64_t* rowind, double* val);
+
+/* Callback applying the remaining skeleton system: Y (n x nrhs, column-major, leading
+ * dimension n, DEVICE memory) holds X(Si,:) of every instance in instance order; the
+ * callback overwrites it with svfun(Y, trans) / mvfun(Y, trans) and returns 0, or returns
+ * nonzero to abort.  Y is valid in stream order on `stream` (the handle's stream); work the
+ * callback enqueues elsewhere must complete before it returns.  trans is 'n' or 'c'. */
+typedef int (*flam_skel_fn)(double* Y, int64_t n, int64_t nrhs, char trans, void* stream, void* ctx);
+
+/* Y = rskelf_partial_sv(F, X, svfun, trans), in place: upward sweep, fn on X(Si,:),
+ * downward sweep.  rskelf/rskelf_partial_sv.m:23-62 ('t' is handled as 'c': real data). */
+FLAM_API flam_status flam_rskelf_partial_sv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans,
+                                            flam_skel_fn fn, void* ctx);
+
+/* Y = rskelf_partial_mv(F, X, mvfun, trans), in place.  rskelf/rskelf_partial_mv.m:23-62. */
+FLAM_API flam_status flam_rskelf_partial_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans,
+                                            flam_skel_fn fn, void* ctx);
+
 /* Sizes of a handle. */
 typedef struct {
   int64_t N;          /* total points */

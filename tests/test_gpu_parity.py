@@ -252,6 +252,9 @@ def test_rskelf_3d_and_covariance(case):
         xo, Ao = x, OK("gaussian", x, dval=1.0 + 1e-4, param=100.0)
         po = OP("annulus", 2, 16, "gaussian", param=100.0, p_rad=16)
         symm, tol, occ = "p", 1e-10, 64
+    # two factorizations within tol of A give solutions within cond(A) * tol of each
+    # other; the Gaussian matrix's diagonal shift 1e-4 puts cond(A) near 1e4
+    amp = 1e4 if case == "gaussian" else 1e3
     F = fb.rskelf(A, x, occ, tol, pxy, dict(symm=symm))
     Fo = o_rskelf(Ao, xo, occ, tol, po, dict(symm=symm), order="level_sync")
     assert [len(f["sk"]) for f in F.factors()["factors"]] == [len(f["sk"]) for f in Fo["factors"]] or \
@@ -260,7 +263,7 @@ def test_rskelf_3d_and_covariance(case):
     B = np.asfortranarray(np.random.default_rng(6).standard_normal((N, 2)))
     X = fb.rskelf_sv(F, B)
     Xo = o_sv(Fo, B)
-    assert np.linalg.norm(X - Xo) / np.linalg.norm(Xo) < 1e3 * tol
+    assert np.linalg.norm(X - Xo) / np.linalg.norm(Xo) < amp * tol
     Ad = Ao.dense()
     assert np.linalg.norm(Ad @ X - B) / np.linalg.norm(B) < 1e4 * tol
 

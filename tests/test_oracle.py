@@ -9,7 +9,8 @@ import pytest
 
 from oracle import configs
 from oracle.idecomp import id_
-from oracle.rskelf import chksymm, chktrans, rskelf, rskelf_mv, rskelf_sv
+from oracle.rskelf import (chksymm, chktrans, rskelf, rskelf_cholmv, rskelf_cholsv, rskelf_logdet, rskelf_mv,
+                           rskelf_partial_info, rskelf_partial_mv, rskelf_partial_sv, rskelf_sv)
 from oracle.snorm import snorm
 from oracle.tree import hypoct, hypoct_perm, mround, tree_arrays
 
@@ -165,6 +166,49 @@ def test_rskelf_partial_factorization():
     x, A, pxy = configs.circle(2048)
     F = rskelf(A, x, 64, 1e-10, pxy, dict(stop=2))
     assert len(F["lvp"]) == 3 and "Si" in F and F["S"].shape == (len(F["Si"]), len(F["Si"]))
+
+
+def test_oracle_cholesky_halves():
+    # F = C C' (rskelf_cholmv.m / rskelf_cholsv.m): C from the downward multiply half
+    N = 700
+    x, A, pxy = configs.circle(N)
+    F = rskelf(A, x, 32, 1e-10, pxy, dict(symm="p"), order="level_sync")
+    I = np.eye(N)
+    C = rskelf_cholmv(F, I)
+    np.testing.assert_allclose(rskelf_cholmv(F, I, "c"), C.T, atol=1e-13)
+    assert np.linalg.norm(C @ C.T - A.dense()) / np.linalg.norm(A.dense()) < 1e-8
+    np.testing.assert_allclose(rskelf_cholsv(F, C), I, atol=1e-12)
+    with pytest.raises(ValueError, match="FLAM:rskelf_cholmv:invalidSymm"):
+        rskelf_cholmv(rskelf(A, x, 32, 1e-10, pxy, dict(symm="n")), I[:, :1])
+
+
+@pytest.mark.parametrize("dval", [1.0, -1.0])
+def test_oracle_logdet(dval):
+    # rskelf_logdet.m: real part = log|det|, imaginary part pi for a negative determinant
+    from oracle.registry import Kernel
+    N = 801
+    x, A0, pxy = configs.star(N, seed=4, clustered=False)
+    A = Kernel("laplace2d", x, scale=A0.scale, dval=dval, weights=A0.weights)
+    F = rskelf(A, x, 32, 1e-10, pxy, dict(symm="n"))
+    ld = rskelf_logdet(F)
+    sign, la = np.linalg.slogdet(A.dense())
+    assert abs(ld.real - la) < 1e-9
+    assert abs(np.exp(1j * ld.imag) - sign) < 1e-9 and 0 <= ld.imag < 2 * math.pi
+
+
+def test_oracle_partial_sv_mv():
+    # rskelf_partial_sv.m / _mv.m with a dense solve of A(Si,Si) + S = full solve
+    N = 1500
+    x, A, pxy = configs.star(N, seed=3, clustered=False)
+    Ad = A.dense()
+    F = rskelf(A, x, 32, 1e-10, pxy, dict(stop=2))
+    Si, S = rskelf_partial_info(F)
+    Ss = Ad[np.ix_(Si, Si)] + S
+    B = np.random.default_rng(1).standard_normal((N, 2))
+    X = rskelf_partial_sv(F, B, lambda Y, t: np.linalg.solve(Ss if t == "n" else Ss.T, Y))
+    assert np.linalg.norm(Ad @ X - B) / np.linalg.norm(B) < 1e-8
+    Y = rskelf_partial_mv(F, B, lambda Z, t: (Ss if t == "n" else Ss.T) @ Z, "t")
+    assert np.linalg.norm(Ad.T @ B - Y) / np.linalg.norm(Ad.T @ B) < 1e-8
 
 
 def test_rskelf_args():
