@@ -990,7 +990,15 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     F.ppool.reserve(std::max<int64_t>(ppool_top, 1), s);
     F.ppool.n = ppool_top;
     mpool[cur].ensure(std::max<int64_t>(mtop, 1), s);
-    etask.upload(et, s);
+    // boxes whose work matrix is in global memory go to the blocked kernel: upload them last
+    std::vector<ElimTask> ets;
+    ets.reserve(nb);
+    for (const ElimTask& e : et)
+      if (e.n <= kSmemN) ets.push_back(e);
+    const int nsmall_e = (int)ets.size();
+    for (const ElimTask& e : et)
+      if (e.n > kSmemN) ets.push_back(e);
+    etask.upload(ets, s);
     chb.upload(ch, s);
     ElimArgs ea{};
     ea.P = P;
@@ -1020,7 +1028,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       }
     }
     if (prof) CK(cudaEventRecord(pe[2], s));
-    launch_eliminate(ea, nb, elim_smem_bytes(nmax_e), s);
+    launch_eliminate(ea, nsmall_e, nb - nsmall_e, elim_smem_bytes(nmax_e), s);
     CK(cudaGetLastError());
     if (prof) CK(cudaEventRecord(pe[3], s));
     if (prof && prof_print) {

@@ -13,6 +13,7 @@
 // end up as K(rd(p),sk).
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tile_f64.cuh"
 
 namespace flam {
 namespace {
@@ -28,6 +29,39 @@ __device__ __forceinline__ AM amax(AM a, AM b) {
   if (b.v > a.v || (b.v == a.v && b.i < a.i)) return b;
   return a;
 }
+
+// Child block of each position of slf: the compress kernel's local permutation
+// maps a position to the concatenated children's skeleton order, and that order
+// locates the entry inside the child's M block (rskelf.m:190-199).
+__device__ __forceinline__ void locate_children(const ElimTask& t, const int32_t* perm, const ChildBlock* ch,
+                                                int* pchild, int* ploc) {
+  for (int q = threadIdx.x; q < t.n; q += kThreads) {
+    const int o = perm[q];
+    int c = -1, loc = 0;
+    for (int b = 0; b < t.nch; ++b)
+      if (o >= ch[b].coff && o < ch[b].coff + ch[b].kc) {
+        c = b;
+        loc = o - ch[b].coff;
+      }
+    pchild[q] = c;
+    ploc[q] = loc;
+  }
+  __syncthreads();
+}
+
+// Entry (i, j) of the children's M blocks placed on the box (0 across children).
+struct MVal {
+  const double* m_in;
+  const ChildBlock* ch;
+  const int* pchild;
+  const int* ploc;
+  __device__ __forceinline__ double operator()(int i, int j) const {
+    const int c = pchild[i];
+    if (c < 0 || c != pchild[j]) return 0.0;
+    const int kc = ch[c].kc;
+    return m_in[ch[c].M_off + ploc[i] + (int64_t)ploc[j] * kc];
+  }
+};
 
 __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
   extern __shared__ __align__(16) double smem[];
@@ -46,26 +80,8 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
   const int64_t* slf = a.ipool + t.slf_off;
   const int32_t* perm = a.permpool + t.perm_off;
   const ChildBlock* ch = a.children + t.ch_first;
-
-  for (int q = tid; q < n; q += kThreads) {
-    const int o = perm[q];
-    int c = -1, loc = 0;
-    for (int b = 0; b < t.nch; ++b)
-      if (o >= ch[b].coff && o < ch[b].coff + ch[b].kc) {
-        c = b;
-        loc = o - ch[b].coff;
-      }
-    pchild[q] = c;
-    ploc[q] = loc;
-  }
-  __syncthreads();
-
-  auto mval = [&](int i, int j) -> double {
-    const int c = pchild[i];
-    if (c < 0 || c != pchild[j]) return 0.0;
-    const int kc = ch[c].kc;
-    return a.m_in[ch[c].M_off + ploc[i] + (int64_t)ploc[j] * kc];
-  };
+  locate_children(t, perm, ch, pchild, ploc);
+  const MVal mval{a.m_in, ch, pchild, ploc};
 
   // 2D loops use a fixed 32 x 8 thread tile: lane = row within a 32-row block
   // (consecutive column-major addresses), warp = column within an 8-column block;
@@ -246,6 +262,266 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
   }
 }
 
+// Boxes with n > kSmemN: the same elimination with the work matrix in global
+// memory (L2-resident) and every O(n^3) part blocked over 32-column panels, so
+// that the bulk of the flops are CTA-wide 64 x 64 tiles (cta_gemm) instead of
+// rank-1 updates:
+//   T updates              two GEMMs (inner dimension k)
+//   LU / chol of K(rd,rd)  right-looking, unblocked 32-column panels (partial
+//                          pivoting as xGETF2 inside the panel; the panel's row
+//                          interchanges then applied to every other column),
+//                          TRSM of the panel's U row block, GEMM trailing update
+//   E, G                   blocked triangular solves: a 32 x 32 diagonal block
+//                          staged in shared memory, GEMM update of the rest
+//   Schur                  one GEMM (E G, or E E' for chol)
+constexpr int kNb = 32;
+
+__global__ void __launch_bounds__(kThreads) k_eliminate_big(ElimArgs a) {
+  __shared__ __align__(16) double tsm[kTileSmemDoubles];
+  __shared__ double blk[kNb * (kNb + 1)];
+  __shared__ AM red[kWarps];
+  __shared__ int s_piv;
+  const ElimTask t = a.tasks[blockIdx.x];
+  const Problem& P = a.P;
+  const InstParams ip = P.ip[t.inst];
+  const int n = t.n, k = t.k, r = n - k;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (n == 0) return;
+  double* K = a.scratch + t.scr_off;                                // n x n, ld n
+  int* pchild = reinterpret_cast<int*>(K + (int64_t)n * n);
+  int* ploc = pchild + n;
+  int* piv = ploc + n;
+  const int64_t* slf = a.ipool + t.slf_off;
+  const int32_t* perm = a.permpool + t.perm_off;
+  const ChildBlock* ch = a.children + t.ch_first;
+  locate_children(t, perm, ch, pchild, ploc);
+  const MVal mval{a.m_in, ch, pchild, ploc};
+  const int tr = lane, tcol = wid;
+  const int64_t ldn = n;
+  if (r == 0) {
+    double* Mo = a.m_out + t.M_out;
+    for (int j = tcol; j < n; j += kWarps)
+      for (int i = tr; i < n; i += 32) Mo[i + (int64_t)j * n] = mval(i, j);
+    return;
+  }
+  for (int j = tcol; j < n; j += kWarps) {
+    const int64_t sj = slf[j];
+    for (int i = tr; i < n; i += 32) K[i + (int64_t)j * n] = aentry(P, ip, slf[i], sj) + mval(i, j);
+  }
+  __syncthreads();
+
+  const double* T = a.tpool + t.T_off;  // k x r, ld k
+  if (k > 0) {
+    // K(rd,:) -= T' K(sk,:);  K(:,rd) -= K(:,sk) T
+    cta_gemm(K + k, 1, ldn, GV{T, k, 1}, GV{K, 1, ldn}, r, n, k, -1.0, tsm);
+    cta_gemm(K + (int64_t)k * n, 1, ldn, GV{K, 1, ldn}, GV{T, 1, k}, n, r, k, -1.0, tsm);
+  }
+
+  double* Kr = K + k + (int64_t)k * n;  // r x r block, ld n
+  auto kr = [&](int i, int j) -> double& { return Kr[i + (int64_t)j * n]; };
+  const bool chol = a.symm == 'p';
+  for (int j0 = 0; j0 < r; j0 += kNb) {
+    const int jb = min(kNb, r - j0), j1 = j0 + jb;
+    if (chol) {
+      for (int j = j0; j < j1; ++j) {
+        const double dj = kr(j, j);
+        if (!(dj > 0.0)) {
+          if (tid == 0) atomicOr(a.status, (int)ST_NOT_SPD);
+          return;
+        }
+        const double lj = sqrt(dj);
+        __syncthreads();
+        for (int q = j + 1 + tid; q < r; q += kThreads) kr(q, j) /= lj;
+        if (tid == 0) kr(j, j) = lj;
+        __syncthreads();
+        for (int c = j + 1 + tcol; c < j1; c += kWarps) {
+          const double lc = kr(c, j);
+          for (int q = c + tr; q < r; q += 32) kr(q, c) -= kr(q, j) * lc;
+        }
+        __syncthreads();
+      }
+      // trailing lower part -= L21 L21'
+      cta_gemm(&kr(j1, j1), 1, ldn, GV{&kr(j1, j0), 1, ldn}, GV{&kr(j1, j0), ldn, 1}, r - j1, r - j1, jb, -1.0,
+               tsm, 1);
+    } else {
+      for (int j = j0; j < j1; ++j) {
+        AM am{-1.0, r};
+        for (int q = j + tid; q < r; q += kThreads) am = amax(am, AM{fabs(kr(q, j)), q});
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          AM b{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+          am = amax(am, b);
+        }
+        if (lane == 0) red[wid] = am;
+        __syncthreads();
+        if (tid == 0) {
+          AM bm = red[0];
+          for (int w = 1; w < kWarps; ++w) bm = amax(bm, red[w]);
+          const int pv0 = (bm.i >= j && bm.i < r) ? bm.i : j;
+          s_piv = pv0;
+          piv[j] = pv0;
+        }
+        __syncthreads();
+        const int pv = (s_piv >= j && s_piv < r) ? s_piv : j;
+        if (pv != j && tid < jb) {  // inside the panel; the other columns after it
+          const double x = kr(j, j0 + tid);
+          kr(j, j0 + tid) = kr(pv, j0 + tid);
+          kr(pv, j0 + tid) = x;
+        }
+        __syncthreads();
+        const double dj = kr(j, j);
+        if (dj != 0.0) {
+          for (int q = j + 1 + tid; q < r; q += kThreads) kr(q, j) /= dj;
+        } else if (tid == 0) {
+          atomicOr(a.status, (int)ST_SINGULAR);
+        }
+        __syncthreads();
+        for (int c = j + 1 + tcol; c < j1; c += kWarps) {
+          const double ujc = kr(j, c);
+          for (int q = j + 1 + tr; q < r; q += 32) kr(q, c) -= kr(q, j) * ujc;
+        }
+        __syncthreads();
+      }
+      // the panel's interchanges on every other column of K (whole rows of K(rd,:))
+      for (int col = tid; col < n; col += kThreads) {
+        if (col >= k + j0 && col < k + j1) continue;
+        double* Kc = K + k + (int64_t)col * n;
+        for (int j = j0; j < j1; ++j) {
+          const int pv = piv[j];
+          if (pv != j) {
+            const double x = Kc[j];
+            Kc[j] = Kc[pv];
+            Kc[pv] = x;
+          }
+        }
+      }
+      // L11 (unit lower) to shared memory
+      for (int e = tid; e < jb * jb; e += kThreads) {
+        const int i = e % jb, c = e / jb;
+        blk[i + c * (kNb + 1)] = kr(j0 + i, j0 + c);
+      }
+      __syncthreads();
+      // U12 = L11 \ A12, one column per thread
+      for (int c = j1 + tid; c < r; c += kThreads) {
+        double x[kNb];
+#pragma unroll
+        for (int i = 0; i < kNb; ++i)
+          if (i < jb) x[i] = kr(j0 + i, c);
+#pragma unroll
+        for (int i = 0; i < kNb; ++i) {
+          if (i < jb) {
+            double v = x[i];
+#pragma unroll
+            for (int l = 0; l < i; ++l) v -= blk[i + l * (kNb + 1)] * x[l];
+            x[i] = v;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < kNb; ++i)
+          if (i < jb) kr(j0 + i, c) = x[i];
+      }
+      __syncthreads();
+      cta_gemm(&kr(j1, j1), 1, ldn, GV{&kr(j1, j0), 1, ldn}, GV{&kr(j0, j1), 1, ldn}, r - j1, r - j1, jb, -1.0, tsm);
+    }
+  }
+
+  // E = K(sk,rd) / U  (U = L' for chol): row-parallel blocked solve
+  if (k > 0) {
+    double* C = K + (int64_t)k * n;   // K(sk, rd): k x r, ld n
+    for (int j0 = 0; j0 < r; j0 += kNb) {
+      const int jb = min(kNb, r - j0), j1 = j0 + jb;
+      for (int e = tid; e < jb * jb; e += kThreads) {   // U(j0+i, j0+c)
+        const int i = e % jb, c = e / jb;
+        blk[i + c * (kNb + 1)] = chol ? kr(j0 + c, j0 + i) : kr(j0 + i, j0 + c);
+      }
+      __syncthreads();
+      for (int row = tid; row < k; row += kThreads) {
+        double x[kNb];
+#pragma unroll
+        for (int c = 0; c < kNb; ++c) {
+          if (c < jb) {
+            double v = C[row + (int64_t)(j0 + c) * n];
+#pragma unroll
+            for (int l = 0; l < c; ++l) v -= x[l] * blk[l + c * (kNb + 1)];
+            x[c] = v / blk[c + c * (kNb + 1)];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < kNb; ++c)
+          if (c < jb) C[row + (int64_t)(j0 + c) * n] = x[c];
+      }
+      __syncthreads();
+      if (j1 < r) {
+        const GV U12 = chol ? GV{&kr(j1, j0), ldn, 1} : GV{&kr(j0, j1), 1, ldn};
+        cta_gemm(C + (int64_t)j1 * n, 1, ldn, GV{C + (int64_t)j0 * n, 1, ldn}, U12, k, r - j1, jb, -1.0, tsm);
+      }
+    }
+    if (!chol) {
+      // G = L \ K(rd(p), sk): column-parallel blocked solve, L unit lower
+      double* Gc = K + k;               // K(rd, sk): r x k, ld n
+      for (int j0 = 0; j0 < r; j0 += kNb) {
+        const int jb = min(kNb, r - j0), j1 = j0 + jb;
+        for (int e = tid; e < jb * jb; e += kThreads) {
+          const int i = e % jb, c = e / jb;
+          blk[i + c * (kNb + 1)] = kr(j0 + i, j0 + c);
+        }
+        __syncthreads();
+        for (int col = tid; col < k; col += kThreads) {
+          double x[kNb];
+#pragma unroll
+          for (int i = 0; i < kNb; ++i) {
+            if (i < jb) {
+              double v = Gc[j0 + i + (int64_t)col * n];
+#pragma unroll
+              for (int l = 0; l < i; ++l) v -= blk[i + l * (kNb + 1)] * x[l];
+              x[i] = v;
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < kNb; ++i)
+            if (i < jb) Gc[j0 + i + (int64_t)col * n] = x[i];
+        }
+        __syncthreads();
+        if (j1 < r)
+          cta_gemm(Gc + j1, 1, ldn, GV{&kr(j1, j0), 1, ldn}, GV{Gc + j0, 1, ldn}, r - j1, k, jb, -1.0, tsm);
+      }
+    }
+  }
+
+  // M_new = M(sk,sk) - E G   (E E' for chol)
+  double* Mo = a.m_out + t.M_out;
+  for (int j = tcol; j < k; j += kWarps)
+    for (int i = tr; i < k; i += 32) Mo[i + (int64_t)j * k] = mval(i, j);
+  __syncthreads();
+  if (k > 0) {
+    const GV E{K + (int64_t)k * n, 1, ldn};
+    const GV Bm = chol ? GV{K + (int64_t)k * n, ldn, 1} : GV{K + k, 1, ldn};
+    cta_gemm(Mo, 1, k, E, Bm, k, k, r, -1.0, tsm);
+  }
+
+  // store the factor: T | LU (or L) | E | G
+  double* F = a.fpool + t.fac_off;
+  const int64_t kr_ = (int64_t)k * r, rr = (int64_t)r * r;
+  for (int64_t e = tid; e < kr_; e += kThreads) F[e] = T[e];
+  for (int j = tcol; j < r; j += kWarps)
+    for (int i = tr; i < r; i += 32) F[kr_ + i + (int64_t)j * r] = (chol && i < j) ? 0.0 : kr(i, j);
+  for (int j = tcol; j < r; j += kWarps)
+    for (int i = tr; i < k; i += 32) F[kr_ + rr + i + (int64_t)j * k] = K[i + (int64_t)(k + j) * n];
+  if (!chol) {
+    for (int j = tcol; j < k; j += kWarps)
+      for (int i = tr; i < r; i += 32) F[2 * kr_ + rr + i + (int64_t)j * r] = K[k + i + (int64_t)j * n];
+    if (tid == 0) {
+      int32_t* pp = a.ppool + t.piv_off;
+      for (int q = 0; q < r; ++q) pp[q] = q;
+      for (int q = 0; q < r; ++q) {
+        const int32_t x = pp[q];
+        pp[q] = pp[piv[q]];
+        pp[piv[q]] = x;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 size_t elim_smem_bytes(int n) {
@@ -255,14 +531,18 @@ size_t elim_smem_bytes(int n) {
 
 int64_t elim_scratch_doubles(int n) { return (int64_t)n * n + (3 * (int64_t)n) / 2 + 2; }
 
-void launch_eliminate(const ElimArgs& a, int ntask, size_t smem, cudaStream_t s) {
-  if (ntask <= 0) return;
+void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_eliminate, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_eliminate<<<ntask, kThreads, smem, s>>>(a);
+  if (nsmall > 0) k_eliminate<<<nsmall, kThreads, smem, s>>>(a);
+  if (nbig > 0) {
+    ElimArgs b = a;
+    b.tasks = a.tasks + nsmall;
+    k_eliminate_big<<<nbig, kThreads, 0, s>>>(b);
+  }
 }
 
 }  // namespace flam

@@ -57,7 +57,8 @@ struct ElimArgs {
 
 size_t elim_smem_bytes(int n);
 int64_t elim_scratch_doubles(int n);
-void launch_eliminate(const ElimArgs& a, int ntask, size_t smem, cudaStream_t s);
+// tasks[0, nsmall): n <= kSmemN (shared-memory kernel); tasks[nsmall, nsmall + nbig): the rest.
+void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cudaStream_t s);
 
 // Segmented copies of int64 ids: dst[dst_off + i] = src[src_off + i], i < len.
 struct CopySeg {
