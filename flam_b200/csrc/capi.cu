@@ -879,7 +879,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // and the per-column kernel for n > kTcMaxN
     auto kkey = [&](int q) {
       const int n = (int)nslf[q];
-      return n <= kTcMaxN ? compress_tc_threads(n) * 8 + compress_tc_group(n) : 0;
+      return n <= kTcMaxN ? compress_tc_threads(n) * 1000 + compress_tc_rows(n) * 10 + compress_tc_group(n) : 0;
     };
     std::vector<int> ord(nb);
     for (int q = 0; q < nb; ++q) ord[q] = q;
@@ -926,7 +926,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       if (key == 0)
         launch_compress(cb, b1 - b0, compress_smem_bytes(nmax_small), s);
       else
-        launch_compress_tc(cb, b1 - b0, key / 8, key % 8, sm, s);
+        launch_compress_tc(cb, b1 - b0, key / 1000, (key / 10) % 100, key % 10, sm, s);
       F.prof.launches += 1;
       b0 = b1;
     }
@@ -1112,13 +1112,22 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   F.t_factor = ms * 1e-3;
   CK(cudaEventDestroy(e0));
   CK(cudaEventDestroy(e1));
+  float gap_elim = 0, gap_next = 0;   // stream time between a step's kernels (host planning)
   for (size_t e = 0; e + 3 < step_ev.size(); e += 4) {
-    float tc = 0, tel = 0;
+    float tc = 0, tel = 0, g = 0;
     CK(cudaEventElapsedTime(&tc, step_ev[e], step_ev[e + 1]));
     CK(cudaEventElapsedTime(&tel, step_ev[e + 2], step_ev[e + 3]));
     F.prof.t_compress += tc * 1e-3;
     F.prof.t_elim += tel * 1e-3;
+    CK(cudaEventElapsedTime(&g, step_ev[e + 1], step_ev[e + 2]));
+    gap_elim += g;
+    if (e + 4 < step_ev.size()) {
+      CK(cudaEventElapsedTime(&g, step_ev[e + 3], step_ev[e + 4]));
+      gap_next += g;
+    }
   }
+  if (prof_print && !step_ev.empty())
+    fprintf(stderr, "[flam] gaps: compress->elim %.3f ms  elim->next compress %.3f ms\n", gap_elim, gap_next);
   for (auto& e : step_ev) CK(cudaEventDestroy(e));
   CK(cudaStreamSynchronize(s));
   if (st & ST_NOT_SPD)

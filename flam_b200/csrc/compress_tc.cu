@@ -58,10 +58,15 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 template <int B, int G>
 __device__ __forceinline__ void reflect_col(double (&p)[B], double al, double* R, int ld, int j, int g,
                                             unsigned gmask, double* vb, double* tau_out) {
-  double sig = 0.0;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;   // four chains: this sum is on the critical path
 #pragma unroll
-  for (int i = 0; i < B; ++i) sig += p[i] * p[i];
-  sig = group_sum<G>(sig, gmask);
+  for (int i = 0; i < B; i += 4) {
+    s0 += p[i] * p[i];
+    s1 += p[i + 1] * p[i + 1];
+    s2 += p[i + 2] * p[i + 2];
+    s3 += p[i + 3] * p[i + 3];
+  }
+  const double sig = group_sum<G>((s0 + s1) + (s2 + s3), gmask);
   double tau = 0.0;
   if (sig != 0.0) {
     const double be = -copysign(sqrt(al * al + sig), al);
@@ -93,7 +98,7 @@ __device__ __forceinline__ double entry_of(const Problem& P, const InstParams& i
 }
 
 template <int B, int G>
-__global__ void __launch_bounds__(B == 32 ? 512 : 1024) k_compress_tc(CompressArgs a) {
+__global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_compress_tc(CompressArgs a) {
   constexpr int PH = B * G;  // panel height
   extern __shared__ __align__(16) double smem[];
   __shared__ Stage<PH> st;
@@ -463,21 +468,33 @@ int64_t compress_tc_doubles(int n) { return (int64_t)n * (n | 1) + 8 * (int64_t)
 
 size_t compress_tc_smem_bytes(int n) { return sizeof(double) * (size_t)compress_tc_doubles(n); }
 
-// Threads per column: 4 for n <= 64, 2 for n <= 256, else 1 (512 threads at most
-// with 32 panel rows per thread; 1024 threads with 16 rows for n > 512).
-int compress_tc_group(int n) { return n <= 64 ? 4 : (n <= 256 ? 2 : 1); }
+// Panel rows per thread (measured on the star-curve workload, N = 262144): 64 for
+// 128 < n <= 256 (one thread per column: 256 threads, so a 64-row column panel fits
+// in registers); 32 for smaller boxes (several threads per column, more CTAs per SM
+// on the levels with thousands of boxes) and up to n = 512; 16 beyond.
+int compress_tc_rows(int n) { return (n > 128 && n <= 256) ? 64 : (n <= 512 ? 32 : 16); }
+
+// Threads per column: with 64 rows per thread 1; with 32 rows 4 for n <= 64, 2 for
+// n <= 256, else 1 (512 threads at most); with 16 rows (n > 512) 1.
+int compress_tc_group(int n) {
+  if (compress_tc_rows(n) == 64) return 1;
+  return n <= 64 ? 4 : (n <= 256 ? 2 : 1);
+}
 
 int compress_tc_threads(int n) {
   int cols = 32;
   while (cols < n) cols <<= 1;
   const int nt = cols * compress_tc_group(n);
-  return nt < 128 && compress_tc_group(n) == 4 ? 128 : nt;
+  return std::max(nt, compress_tc_rows(n) * compress_tc_group(n));   // at least one thread per panel row
 }
 
-void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int g, size_t smem, cudaStream_t s) {
+void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, size_t smem, cudaStream_t s) {
   if (ntask <= 0) return;
-  if (nt > 512)
+  if (b == 16)
     launch_b<16, 1>(a, ntask, nt, smem, s);
+  else if (b == 64)
+    g == 4 ? launch_b<64, 4>(a, ntask, nt, smem, s)
+           : (g == 2 ? launch_b<64, 2>(a, ntask, nt, smem, s) : launch_b<64, 1>(a, ntask, nt, smem, s));
   else if (g == 4)
     launch_b<32, 4>(a, ntask, nt, smem, s);
   else if (g == 2)

@@ -37,7 +37,8 @@ int64_t compress_tc_doubles(int n);
 size_t compress_tc_smem_bytes(int n);
 int compress_tc_threads(int n);
 int compress_tc_group(int n);
-void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int g, size_t smem, cudaStream_t s);
+int compress_tc_rows(int n);
+void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, size_t smem, cudaStream_t s);
 
 struct ElimArgs {
   Problem P;
