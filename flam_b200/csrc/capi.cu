@@ -153,7 +153,7 @@ struct LevelStat {
 struct Workspace {
   DBuf<int64_t> cpool;
   DBuf<double> tpool, scratch, mpool[2], W, tmp;
-  DBuf<int32_t> permpool, status;
+  DBuf<int32_t> permpool, status, mfilt;
   DBuf<CompressTask> ctask;
   DBuf<ElimTask> etask;
   DBuf<ChildBlock> chb;
@@ -164,6 +164,7 @@ struct Workspace {
     cpool.release(s);
     permpool.release(s);
     status.release(s);
+    mfilt.release(s);
     ctask.release(s);
     etask.release(s);
     chb.release(s);
@@ -829,6 +830,13 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // ---- tasks
     std::vector<CompressTask> ct(nb);
     std::vector<int64_t> elim_scr(nb, -1);
+    // Row-split form on the levels with few boxes: each large box's rows go to
+    // nparts CTAs whose R factors are then merged pairwise, so that the step
+    // occupies more of the GPU's 148 SMs.
+    int nparts = 1;
+    if (nb <= 74)
+      while (nparts * 2 <= 8 && nparts * 2 * nb <= 148) nparts *= 2;
+    std::vector<char> split(nb, 0);
     int64_t ttop = 0, ptop = 0, stop_s = 0;
     int nmax_small = 0;
     for (int q = 0; q < nb; ++q) {
@@ -856,12 +864,17 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       // shared by the compress and elimination kernels of this step
       const int n = (int)nslf[q];
       const bool tc = n <= kTcMaxN;
-      const bool c_glob = tc ? compress_tc_smem_bytes(n) > tc_smem_max() : n > kSmemN;
+      const int64_t mcap = (F.symm == 'n' ? 2 : 1) * ncand[q] +
+                           (use_proxy ? (F.iph[i].two_sided ? 2 : 1) * (int64_t)F.npxy : 0);
+      split[q] = nparts > 1 && tc && n > 128 && mcap >= 64 * nparts;
+      const bool c_glob = split[q] || (tc ? compress_tc_smem_bytes(n) > tc_smem_max() : n > kSmemN);
       const bool e_glob = n > kSmemN;
       t.scr_off = -1;
       elim_scr[q] = -1;
       if (c_glob || e_glob) {
-        const int64_t slot = std::max(tc ? compress_tc_doubles(n) : compress_scratch_doubles(n), elim_scratch_doubles(n));
+        const int64_t cslot = split[q] ? nparts * compress_tc_doubles(n)
+                                       : (tc ? compress_tc_doubles(n) : compress_scratch_doubles(n));
+        const int64_t slot = std::max(cslot, elim_scratch_doubles(n));
         if (c_glob) t.scr_off = stop_s;
         if (e_glob) elim_scr[q] = stop_s;
         stop_s += slot;
@@ -877,17 +890,51 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     launch_gather_ids(F.ipool.p, cpool.p, csegs.p, (int)cs.size(), s);
     // group the boxes by kernel shape: thread-per-column blocks of 32..1024 threads,
     // and the per-column kernel for n > kTcMaxN
-    auto kkey = [&](int q) {
-      const int n = (int)nslf[q];
+    auto kkey_n = [](int n) {
       return n <= kTcMaxN ? compress_tc_threads(n) * 1000 + compress_tc_rows(n) * 10 + compress_tc_group(n) : 0;
     };
-    std::vector<int> ord(nb);
-    for (int q = 0; q < nb; ++q) ord[q] = q;
+    auto kkey = [&](int q) { return kkey_n((int)nslf[q]); };
+    std::vector<int> ord;
+    for (int q = 0; q < nb; ++q)
+      if (!split[q]) ord.push_back(q);
     std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return kkey(x) < kkey(y); });
-    std::vector<CompressTask> cts(nb);
-    for (int q = 0; q < nb; ++q) cts[q] = ct[ord[q]];
+    // task segments: [whole boxes | filter of split boxes | parts | merge level 0 | level 1 ...]
+    std::vector<CompressTask> cts;
+    cts.reserve(nb * 3);
+    for (int q : ord) cts.push_back(ct[q]);
+    std::vector<int> seg{(int)cts.size()};
+    std::vector<int> sord;
+    for (int q = 0; q < nb; ++q)
+      if (split[q]) sord.push_back(q);
+    std::stable_sort(sord.begin(), sord.end(), [&](int x, int y) { return kkey(x) < kkey(y); });
+    if (!sord.empty()) {
+      for (int q : sord) cts.push_back(ct[q]);
+      seg.push_back((int)cts.size());
+      for (int q : sord)
+        for (int pt = 0; pt < nparts; ++pt) {
+          CompressTask u = ct[q];
+          u.mode = 1;
+          u.part = pt;
+          u.nparts = nparts;
+          u.scr_off = ct[q].scr_off + pt * compress_tc_doubles(u.n);
+          cts.push_back(u);
+        }
+      seg.push_back((int)cts.size());
+      for (int h = 1; h < nparts; h *= 2) {
+        for (int q : sord)
+          for (int pt = 0; pt < nparts; pt += 2 * h) {
+            CompressTask u = ct[q];
+            u.mode = 2 * h == nparts ? 3 : 2;
+            u.scr_off = ct[q].scr_off + pt * compress_tc_doubles(u.n);
+            u.rsrc_off = ct[q].scr_off + (pt + h) * compress_tc_doubles(u.n);
+            cts.push_back(u);
+          }
+        seg.push_back((int)cts.size());
+      }
+    }
     ctask.upload(cts, s);
     cout.ensure(nb, s);
+    ws.mfilt.ensure(nb, s);
     CompressArgs ca{};
     ca.P = P;
     ca.tasks = ctask.p;
@@ -904,6 +951,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ca.rrqr_iter = o.rrqr_iter;
     ca.Aexp = nullptr;
     ca.lda = 0;
+    ca.mfilt = ws.mfilt.p;
     F.prof.launches += 2 + 1;  // two id gathers, compress
     F.prof.n_compress += 1;
     if (prof) {
@@ -913,22 +961,33 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       pe = step_ev.data() + base;
       CK(cudaEventRecord(pe[0], s));
     }
-    for (int b0 = 0; b0 < nb;) {
-      const int key = kkey(ord[b0]);
-      int b1 = b0;
-      size_t sm = 16;
-      while (b1 < nb && kkey(ord[b1]) == key) {
-        if (key > 0 && cts[b1].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(cts[b1].n));
-        ++b1;
+    // one launch per kernel shape within a segment of the task array
+    auto launch_segment = [&](int t0, int t1) {
+      for (int b0 = t0; b0 < t1;) {
+        const int key = kkey_n(cts[b0].n);
+        int b1 = b0;
+        size_t sm = 16;
+        while (b1 < t1 && kkey_n(cts[b1].n) == key) {
+          if (key > 0 && cts[b1].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(cts[b1].n));
+          ++b1;
+        }
+        CompressArgs cb = ca;
+        cb.tasks = ctask.p + b0;
+        if (key == 0)
+          launch_compress(cb, b1 - b0, compress_smem_bytes(nmax_small), s);
+        else
+          launch_compress_tc(cb, b1 - b0, key / 1000, (key / 10) % 100, key % 10, sm, s);
+        F.prof.launches += 1;
+        b0 = b1;
       }
-      CompressArgs cb = ca;
-      cb.tasks = ctask.p + b0;
-      if (key == 0)
-        launch_compress(cb, b1 - b0, compress_smem_bytes(nmax_small), s);
-      else
-        launch_compress_tc(cb, b1 - b0, key / 1000, (key / 10) % 100, key % 10, sm, s);
+    };
+    launch_segment(0, seg[0]);
+    if (seg.size() > 1) {
+      CompressArgs cf = ca;
+      cf.tasks = ctask.p + seg[0];
+      launch_filter(cf, seg[1] - seg[0], s);
       F.prof.launches += 1;
-      b0 = b1;
+      for (size_t g = 1; g + 1 < seg.size(); ++g) launch_segment(seg[g], seg[g + 1]);
     }
     F.prof.launches -= 1;
     CK(cudaGetLastError());

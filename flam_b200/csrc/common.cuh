@@ -67,6 +67,15 @@ struct CompressTask {
   int32_t out_idx;   // slot of this box in the CompressOut array
   double ctr[kMaxDim];
   double l[kMaxDim];
+  // Row-split form for boxes of the few-box levels: the rows of K are divided into
+  // nparts parts whose R factors are merged pairwise.  mode 0: the whole ID in one
+  // CTA; 1: R of rows [part*m/nparts, (part+1)*m/nparts) into this task's R area;
+  // 2: fold the triangular R at rsrc_off into this task's R (merge); 3: as 2, then
+  // the rest of the ID.  Modes 1-3 read the filtered candidate count from mfilt.
+  int32_t mode;
+  int32_t part, nparts;
+  int32_t pad_;
+  int64_t rsrc_off;
 };
 
 // Per-box results of the compress kernel.

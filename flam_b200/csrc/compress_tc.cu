@@ -97,6 +97,56 @@ __device__ __forceinline__ double entry_of(const Problem& P, const InstParams& i
   }
 }
 
+// pxyfun's neighbour selection (the reference test drivers' filters): stable
+// compaction of the box's candidate list in place; returns the kept count.
+__device__ __forceinline__ int filter_candidates(const CompressTask& t, const Problem& P, const InstParams& ip,
+                                                 int64_t* cand, int* s_cnt) {
+  const int NT = blockDim.x, nw = NT >> 5, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int d = P.d;
+  int total = 0;
+  for (int c0 = 0; c0 < t.ncand; c0 += NT) {
+    const int ci = c0 + tid;
+    int64_t q = -1;
+    bool keep = false;
+    if (ci < t.ncand) {
+      q = cand[ci];
+      const double* xq = P.x + q * d;
+      if (ip.pkind == P_ANNULUS) {
+        double mx = 0.0;
+        for (int k = 0; k < d; ++k) mx = fmax(mx, __ddiv_rn(fabs(__dsub_rn(xq[k], t.ctr[k])), t.l[k]));
+        keep = mx < 1.5;
+      } else {
+        double s = 0.0;
+        for (int k = 0; k < d; ++k) {
+          const double z = __ddiv_rn(__dsub_rn(xq[k], t.ctr[k]), t.l[k]);
+          s = __dadd_rn(s, __dmul_rn(z, z));
+        }
+        keep = s < 2.25;
+      }
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_cnt[wid] = __popc(bal);
+    __syncthreads();
+    int pre = total, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < wid) pre += s_cnt[w];
+      tot += s_cnt[w];
+    }
+    if (keep) cand[pre + __popc(bal & ((1u << lane) - 1u))] = q;
+    total += tot;
+    __syncthreads();
+  }
+  return total;
+}
+
+__global__ void __launch_bounds__(256) k_filter(CompressArgs a) {
+  __shared__ int s_cnt[8];
+  const CompressTask t = a.tasks[blockIdx.x];
+  const InstParams ip = a.P.ip[t.inst];
+  const int m1 = (t.flags & 2) ? filter_candidates(t, a.P, ip, a.cpool + t.cand_off, s_cnt) : t.ncand;
+  if (threadIdx.x == 0) a.mfilt[t.out_idx] = m1;
+}
+
 template <int B, int G>
 __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_compress_tc(CompressArgs a) {
   constexpr int PH = B * G;  // panel height
@@ -130,59 +180,37 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   double* aux = vn2 + n;                                         // 6n (RRQR), reused for ids
   int* jpvt = reinterpret_cast<int*>(aux + 6 * (int64_t)n);
 
-  // ---- (1) neighbour filter (pxyfun's nbr selection), stable compaction in place
-  int m1 = t.ncand;
-  if (t.flags & 2) {
-    int total = 0;
-    for (int c0 = 0; c0 < t.ncand; c0 += NT) {
-      const int ci = c0 + tid;
-      int64_t q = -1;
-      bool keep = false;
-      if (ci < t.ncand) {
-        q = cand[ci];
-        const double* xq = P.x + q * d;
-        if (ip.pkind == P_ANNULUS) {
-          double mx = 0.0;
-          for (int k = 0; k < d; ++k) mx = fmax(mx, __ddiv_rn(fabs(__dsub_rn(xq[k], t.ctr[k])), t.l[k]));
-          keep = mx < 1.5;
-        } else {
-          double s = 0.0;
-          for (int k = 0; k < d; ++k) {
-            const double z = __ddiv_rn(__dsub_rn(xq[k], t.ctr[k]), t.l[k]);
-            s = __dadd_rn(s, __dmul_rn(z, z));
-          }
-          keep = s < 2.25;
-        }
-      }
-      const unsigned bal = __ballot_sync(0xffffffffu, keep);
-      if (lane == 0) s_cnt[wid] = __popc(bal);
-      __syncthreads();
-      int pre = total, tot = 0;
-      for (int w = 0; w < nw; ++w) {
-        if (w < wid) pre += s_cnt[w];
-        tot += s_cnt[w];
-      }
-      if (keep) cand[pre + __popc(bal & ((1u << lane) - 1u))] = q;
-      total += tot;
-      __syncthreads();
-    }
-    m1 = total;
-  }
+  // ---- (1) neighbour filter (pxyfun's nbr selection), stable compaction in place;
+  // the row-split parts read the count the filter launch left
+  const int mode = t.mode;
+  const int m1 = mode != 0 ? a.mfilt[t.out_idx] : ((t.flags & 2) ? filter_candidates(t, P, ip, cand, s_cnt) : t.ncand);
   const int nrep = a.symm_n ? 2 : 1;
   const int npr = (t.flags & 1) ? (ip.two_sided ? 2 * P.npxy : P.npxy) : 0;
   const int m = a.Aexp ? t.ncand : nrep * m1 + npr;
   const int mn = min(m, n);
 
-  // ---- (2) TSQR: fold PH-row panels of K into R0; G threads per column
-  for (int64_t e = tid; e < (int64_t)n * ld; e += NT) R[e] = 0.0;
+  // ---- (2) TSQR: fold PH-row panels of K into R0; G threads per column.  A part of
+  // the row-split form folds rows [rbeg, rend) of K; a merge folds the rows of the
+  // upper triangular R at rsrc_off into the R already in place.
+  int rbeg = 0, rend = m;
+  const double* Rsrc = nullptr;
+  if (mode == 1) {
+    rbeg = (int)((int64_t)t.part * m / t.nparts);
+    rend = (int)((int64_t)(t.part + 1) * m / t.nparts);
+  } else if (mode >= 2) {
+    Rsrc = a.scratch + t.rsrc_off;
+    rend = n;
+  }
+  if (mode < 2)
+    for (int64_t e = tid; e < (int64_t)n * ld; e += NT) R[e] = 0.0;
   const int col = tid / G, g = tid % G;
   const unsigned gmask = (G == 1) ? (1u << lane) : (((1u << G) - 1u) << (lane & ~(G - 1)));
   const int64_t sc = col < n ? slf[col] : 0;
   __syncthreads();
   double p[B];
-  for (int p0 = 0; p0 < m; p0 += PH) {
-    if (!a.Aexp && tid < PH) {
-      const int rho = p0 + tid;
+  for (int p0 = rbeg; p0 < rend; p0 += PH) {
+    if (!a.Aexp && !Rsrc && tid < PH) {
+      const int rho = p0 + tid < rend ? p0 + tid : m;   // rows past the part are zero
       int ty = 3;
       int64_t q = -1;
       double wm = 0.0;
@@ -211,7 +239,10 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     __syncthreads();
     if (col < n) {
       const int r0 = p0 + g * B;
-      if (a.Aexp) {
+      if (Rsrc) {
+#pragma unroll
+        for (int i = 0; i < B; ++i) p[i] = (r0 + i < rend) ? Rsrc[(int64_t)(r0 + i) * ld + col] : 0.0;
+      } else if (a.Aexp) {
 #pragma unroll
         for (int i = 0; i < B; ++i) p[i] = (r0 + i < m) ? a.Aexp[(r0 + i) + (int64_t)col * a.lda] : 0.0;
       } else {
@@ -222,13 +253,15 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         }
       }
     }
-    // reflector 0 of this panel, formed by its owners.  Thread col is the only
+    // first reflector of this panel, formed by its owners.  Thread col is the only
     // writer of column col of R, so it reads R(j+1, col) one reflector ahead
-    // (the load overlaps step j and its barrier).
-    double rcur = col < n ? R[col] : 0.0;   // R(0, col)
-    if (col == 0) reflect_col<B, G>(p, rcur, R, ld, 0, g, gmask, vbuf[0], &tau2[0]);
+    // (the load overlaps step j and its barrier).  Rows p0.. of a triangular R are
+    // zero left of column p0: those reflectors are the identity and are skipped.
+    const int js = Rsrc ? p0 : 0;
+    double rcur = col < n ? R[(int64_t)js * ld + col] : 0.0;   // R(js, col)
+    if (col == js) reflect_col<B, G>(p, rcur, R, ld, js, g, gmask, vbuf[js & 1], &tau2[js & 1]);
     __syncthreads();
-    for (int j = 0; j < n; ++j) {
+    for (int j = js; j < n; ++j) {
       const int b = j & 1;
       const double rnext = (col > j && col < n && j + 1 < n) ? R[(int64_t)(j + 1) * ld + col] : 0.0;
       const double tau = tau2[b];
@@ -253,6 +286,8 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
       __syncthreads();
     }
   }
+
+  if (mode == 1 || mode == 2) return;   // this part's R stays in place for the next merge
 
   // ---- (3) column-pivoted QR of R0 (xLAQP2) for min(m, n) steps
   if (c < n) {
@@ -486,6 +521,10 @@ int compress_tc_threads(int n) {
   while (cols < n) cols <<= 1;
   const int nt = cols * compress_tc_group(n);
   return std::max(nt, compress_tc_rows(n) * compress_tc_group(n));   // at least one thread per panel row
+}
+
+void launch_filter(const CompressArgs& a, int ntask, cudaStream_t s) {
+  if (ntask > 0) k_filter<<<ntask, 256, 0, s>>>(a);
 }
 
 void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, size_t smem, cudaStream_t s) {

@@ -20,6 +20,7 @@ struct CompressArgs {
   int64_t rrqr_iter;   // < 0: unlimited
   const double* Aexp;  // explicit m x n matrix (flam_id); rows are generated from points when null
   int64_t lda;
+  int32_t* mfilt;      // per box (out_idx): candidates kept by the neighbour filter (row-split form)
 };
 
 size_t compress_smem_bytes(int n);
@@ -39,6 +40,9 @@ int compress_tc_threads(int n);
 int compress_tc_group(int n);
 int compress_tc_rows(int n);
 void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, size_t smem, cudaStream_t s);
+// Neighbour filter alone (row-split form): tasks[0, ntask) compact their candidates
+// and write the kept count to a.mfilt[out_idx].
+void launch_filter(const CompressArgs& a, int ntask, cudaStream_t s);
 
 struct ElimArgs {
   Problem P;
