@@ -833,9 +833,16 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // Row-split form on the levels with few boxes: each large box's rows go to
     // nparts CTAs whose R factors are then merged pairwise, so that the step
     // occupies more of the GPU's 148 SMs.
+    static const int split_ctas = [] {   // CTAs a split step aims at (tuning: FLAM_SPLIT_CTAS)
+      const char* e = std::getenv("FLAM_SPLIT_CTAS");
+      return e ? std::max(1, std::atoi(e)) : 148;
+    }();
+    static const int split_max = [] {    // parts per box at most (FLAM_SPLIT_MAX)
+      const char* e = std::getenv("FLAM_SPLIT_MAX");
+      return e ? std::max(1, std::atoi(e)) : 8;
+    }();
     int nparts = 1;
-    if (nb <= 74)
-      while (nparts * 2 <= 8 && nparts * 2 * nb <= 148) nparts *= 2;
+    while (nparts * 2 <= split_max && nparts * 2 * nb <= split_ctas) nparts *= 2;
     std::vector<char> split(nb, 0);
     int64_t ttop = 0, ptop = 0, stop_s = 0;
     int nmax_small = 0;
