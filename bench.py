@@ -34,6 +34,11 @@ METRIC = "rskelf factor+solve DOF/s at 1e-10 rel. err: chosen form vs plain FP64
 UNIT = "DOF/s"
 N_DEF, NRHS_DEF, OCC, TOL = 262144, 256, 64, 1e-10
 CPU_SAMPLE_N = 16384
+# DRAM bytes (read + write) per compress step of the N=262144 workload: one ncu capture
+# of every k_compress_tc launch of an N=65536 factorization (130.4 MB over its level
+# steps; profiles/k_compress_tc_star65536_top.md) scaled by the box count (x4) and
+# divided by this workload's 23 steps.
+COMPRESS_TRAFFIC_PER_STEP = 4 * 130.4e6 / 23
 
 
 def parse():
@@ -288,7 +293,9 @@ def main():
     kernel_name = {"compress": "k_compress (fused proxy filter + assembly + TSQR + CPQR + RRQR)",
                    "elim": "k_eliminate", "sweep": "k_sweep"}[top]
     roofline = {"kernel": kernel_name, "bound": "fp64", "achieved": achieved, "peak": peak_fp64,
-                "unit": "TFLOP/s", "frac": achieved / peak_fp64 if peak_fp64 else None, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak_fp64 if peak_fp64 else None,
+                "traffic": COMPRESS_TRAFFIC_PER_STEP if top == "compress" and args.n == N_DEF else None,
+                "traffic_unit": "bytes per step launch group (ncu capture at N=65536 scaled x4)",
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "launches": n_k, "avg_launch_ms": t_k / max(n_k, 1) * 1e3,
                 "algorithmic_flop_per_launch": f_k / max(n_k, 1),
