@@ -8,7 +8,8 @@ from ._lib import FlamError, lib
 from .api import (Factor, hypoct, hypoct_perm, id, rskelf, rskelf_batched, rskelf_cholmv, rskelf_cholsv,
                   rskelf_logdet, rskelf_mv, rskelf_partial_info, rskelf_partial_mv, rskelf_partial_sv, rskelf_sv)
 from .registry import Kernel, Proxy
-from . import problems
+from . import problems, shard
 
 __all__ = ["FlamError", "lib", "Factor", "hypoct", "hypoct_perm", "id", "rskelf", "rskelf_batched", "rskelf_mv",
-           "rskelf_sv", "Kernel", "Proxy", "problems"]
+           "rskelf_sv", "rskelf_cholmv", "rskelf_cholsv", "rskelf_logdet", "rskelf_partial_info",
+           "rskelf_partial_sv", "rskelf_partial_mv", "Kernel", "Proxy", "problems", "shard"]
