@@ -395,6 +395,52 @@ class _DevBlock:
                                          "version": 2, "strides": (8, 8 * n)}
 
 
+def factor_import(F, stream=None):
+    """Device handle from a factorization in the reference's F layout (rskelf.m:157-159,
+    249-257): a dict with N, symm and factors, each factor a dict of sk, rd (0-based), T,
+    L, U, p, E, F (U, p, F unused for symm 'p').  Factorizations made elsewhere in rskelf
+    format -- hifie2/hifie3, whose hifie_sv/mv are rskelf_sv/mv on that F
+    (hifie/hifie_sv.m:21), or one saved from MATLAB -- then run rskelf_sv/mv/cholsv/cholmv/
+    logdet on the device.  Factors act in list order."""
+    symm = str(F["symm"]).lower()
+    fs = F["factors"]
+    chol = symm == "p"
+    ks = np.array([len(f["sk"]) for f in fs], dtype=np.int64)
+    rs = np.array([len(f["rd"]) for f in fs], dtype=np.int64)
+
+    def cat(key, shape, dtype=np.float64):
+        parts = []
+        for f, k, r in zip(fs, ks, rs):
+            a = np.asarray(f[key], dtype=dtype)
+            parts.append(np.asfortranarray(a.reshape(shape(k, r))).ravel(order="F"))
+        return np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(0, dtype))
+
+    i64 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))  # noqa: E731
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    sk = cat("sk", lambda k, r: (k,), np.int64)
+    rd = cat("rd", lambda k, r: (r,), np.int64)
+    T = cat("T", lambda k, r: (k, r))
+    L = cat("L", lambda k, r: (r, r))
+    E = cat("E", lambda k, r: (k, r))
+    U = p = G = None
+    if not chol:
+        U = cat("U", lambda k, r: (r, r))
+        p = cat("p", lambda k, r: (r,), np.int64)
+        G = cat("F", lambda k, r: (r, k))
+    h = C.c_void_p()
+    nf = len(fs)
+    z = np.zeros(1)
+    zi = np.zeros(1, np.int64)
+    _lib.check(_lib.lib().flam_factor_import(
+        int(F["N"]), symm.encode()[:1], nf, i64(ks if nf else zi), i64(rs if nf else zi), i64(sk if sk.size else zi),
+        i64(rd if rd.size else zi), dp(T if T.size else z), dp(L if L.size else z),
+        None if U is None else dp(U if U.size else z), None if p is None else i64(p if p.size else zi),
+        dp(E if E.size else z), None if G is None else dp(G if G.size else z), stream, C.byref(h)))
+    out = Factor(h.value, 1)
+    out._sizes = [int(F["N"])]
+    return out
+
+
 def hypoct(x, occ, lvlmax=math.inf, ext=None):
     """T = hypoct(x, occ, lvlmax, ext), built on the device.   core/hypoct.m:51-171."""
     x = np.asfortranarray(x, dtype=np.float64)

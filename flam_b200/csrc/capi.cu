@@ -245,7 +245,8 @@ struct flam_factor {
 
   ~flam_factor() {
     resolve_pending();
-    if (!s && !x.p) return;
+    const bool any = x.p || ipool.p || fpool.p || ppool.p || hperm.p || ip.p || !steps.empty();
+    if (!any) return;   // nothing on the device (e.g. a handle that failed before its uploads)
     cudaStream_t st = s;
     x.release(st);
     w.release(st);
@@ -1923,6 +1924,120 @@ flam_status flam_factor_export(const flam_factor* F, int inst, int64_t j, int64_
         for (int64_t q = 0; q < r; ++q) p[q] = pv[q];
       }
     }
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_factor_import(int64_t N, char symm, int64_t nfac, const int64_t* k, const int64_t* r,
+                               const int64_t* sk, const int64_t* rd, const double* T, const double* L,
+                               const double* U, const int64_t* p, const double* E, const double* G, void* stream,
+                               flam_factor** F) {
+  return guard([&] {
+    if (!F) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: output handle pointer is NULL");
+    *F = nullptr;
+    symm = chksymm(symm);
+    if (symm == 'h') fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h' is not built on the device");
+    const bool chol = symm == 'p';
+    if (N < 0 || nfac < 0) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: negative size");
+    if (nfac > 0 && (!k || !r || !sk || !rd || !T || !L || !E || (!chol && (!U || !p || !G))))
+      fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: a factor array is NULL");
+    // host images of the pools; groups of consecutive factors with disjoint index sets
+    std::vector<int64_t> ids;
+    std::vector<double> fp;
+    std::vector<int32_t> pp;
+    std::vector<std::vector<FacDesc>> groups(1);
+    std::vector<HostFac> hf;
+    std::vector<int64_t> gstamp((size_t)N, -1), fstamp((size_t)N, -1);
+    int64_t g = 0, ko = 0, ro = 0, kro = 0, rro = 0, ntot_r = 0;
+    for (int64_t j = 0; j < nfac; ++j) {
+      const int64_t kj = k[j], rj = r[j];
+      if (kj < 0 || rj < 0 || kj > N || rj > N) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: bad factor size");
+      bool clash = false;
+      for (int64_t q = 0; q < kj + rj; ++q) {
+        const int64_t v = q < kj ? sk[ko + q] : rd[ro + q - kj];
+        if (v < 0 || v >= N) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: factor %lld: index outside [0, N)", (long long)j);
+        if (fstamp[v] == j) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: factor %lld: repeated index", (long long)j);
+        fstamp[v] = j;
+        clash |= gstamp[v] == g;
+      }
+      if (rj > 0) {
+        if (clash) {
+          groups.emplace_back();
+          ++g;
+        }
+        for (int64_t q = 0; q < kj + rj; ++q) gstamp[q < kj ? sk[ko + q] : rd[ro + q - kj]] = g;
+        const int64_t kr = kj * rj, rr = rj * rj;
+        FacDesc f{};
+        f.sk_off = (int64_t)ids.size();
+        for (int64_t q = 0; q < kj; ++q) ids.push_back(sk[ko + q]);
+        for (int64_t q = 0; q < rj; ++q) ids.push_back(rd[ro + q]);
+        const int64_t off = (int64_t)fp.size();
+        f.T_off = off;
+        f.LU_off = off + kr;
+        f.E_off = off + kr + rr;
+        f.G_off = off + 2 * kr + rr;
+        fp.insert(fp.end(), T + kro, T + kro + kr);
+        for (int64_t c = 0; c < rj; ++c)       // [L\U] (unit L implicit) or the Cholesky factor
+          for (int64_t q = 0; q < rj; ++q)
+            fp.push_back(chol ? (q >= c ? L[rro + q + c * rj] : 0.0)
+                              : (q > c ? L[rro + q + c * rj] : U[rro + q + c * rj]));
+        fp.insert(fp.end(), E + kro, E + kro + kr);
+        f.piv_off = (int64_t)pp.size();
+        if (!chol) {
+          fp.insert(fp.end(), G + kro, G + kro + kr);
+          for (int64_t q = 0; q < rj; ++q) {
+            if (p[ro + q] < 0 || p[ro + q] >= rj)
+              fail(FLAM_ERR_ARG, "FLAM:gpu:invalidFactor: factor %lld: permutation entry outside [0, r)",
+                   (long long)j);
+            pp.push_back((int32_t)p[ro + q]);
+          }
+        }
+        f.k = (int32_t)kj;
+        f.r = (int32_t)rj;
+        groups[g].push_back(f);
+        hf.push_back(HostFac{0, (int)g, f.sk_off, f.k, f.r, off, f.piv_off});
+        ntot_r += rj;
+      }
+      ko += kj;
+      ro += rj;
+      kro += kj * rj;
+      rro += rj * rj;
+    }
+    std::unique_ptr<flam_factor> H(new flam_factor());
+    CK(cudaGetDevice(&H->dev));
+    H->s = (cudaStream_t)stream;
+    H->d = 0;
+    H->ninst = 1;
+    H->inst_off = {0, N};
+    H->Ntot = N;
+    H->symm = symm;
+    H->ipool.upload(ids, H->s);
+    H->fpool.upload(fp, H->s);
+    H->ppool.upload(pp, H->s);
+    H->hfac = hf;
+    H->inst_fac.assign(1, {});
+    H->inst_lvp.assign(1, {0});
+    for (size_t q = 0; q < hf.size(); ++q) H->inst_fac[0].push_back((int64_t)q);
+    for (auto& grp : groups) {
+      if (grp.empty()) continue;
+      StepDev sd;
+      sd.fac.upload(grp, H->s);
+      sd.nfac = (int)grp.size();
+      for (const FacDesc& f : grp) {
+        sd.kmax = std::max(sd.kmax, f.k);
+        sd.rmax = std::max(sd.rmax, f.r);
+        sd.flop_per_rhs += 4.0 * f.k * f.r + (double)f.r * f.r;
+        sd.fac_bytes += 8.0 * (2.0 * f.k * f.r + (double)f.r * f.r);
+        sd.x_rows += f.k + f.r;
+      }
+      H->steps.push_back(std::move(sd));
+      H->inst_lvp[0].push_back(H->inst_lvp[0].back() + (int64_t)grp.size());
+    }
+    H->rem.assign(1, N - ntot_r);
+    H->stats.assign(1, {});
+    H->nlvl.assign(1, 0);
+    CK(cudaStreamSynchronize(H->s));
+    *F = H.release();
     return FLAM_OK;
   });
 }

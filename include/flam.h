@@ -189,6 +189,24 @@ FLAM_API flam_status flam_partial_sizes(const flam_factor* F, int inst, int64_t*
 FLAM_API flam_status flam_partial_export(const flam_factor* F, int inst, int64_t* Si, int64_t* colptr,
                                          int64_t* rowind, double* val);
 
+/* Device handle from a factorization given on the host in the reference's F layout
+ * (rskelf.m:157-159,249-257): N, symm and factors(1..nfac) in application order, sk and rd
+ * 0-based.  Factorizations produced elsewhere in rskelf format are applied this way: the
+ * hifie2/hifie3 factorizations, whose hifie_sv/mv/cholsv/cholmv/logdet are rskelf_sv/...
+ * on that F (hifie/hifie_sv.m:21), or a factorization saved from a MATLAB session.
+ * Factor j (k_j = |sk|, r_j = |rd|) occupies, one factor after another: sk (k_j), rd (r_j),
+ * T (k_j x r_j), L (r_j x r_j), U (r_j x r_j; NULL for 'p'), p (r_j; NULL for 'p'),
+ * E (k_j x r_j), G (r_j x k_j, the reference's field F; NULL for 'p'), column-major.
+ * Consecutive factors with disjoint index sets are applied in one launch; a factor that
+ * touches an index of the current group starts the next, so the factors act in the
+ * reference's loop order.  symm 'n', 's' or 'p'; the handle runs on `stream`.
+ * Errors: FLAM:gpu:invalidFactor (an index outside [0, N), repeated inside a factor, a
+ * permutation entry outside [0, r), a missing array). */
+FLAM_API flam_status flam_factor_import(int64_t N, char symm, int64_t nfac, const int64_t* k, const int64_t* r,
+                                        const int64_t* sk, const int64_t* rd, const double* T, const double* L,
+                                        const double* U, const int64_t* p, const double* E, const double* G,
+                                        void* stream, flam_factor** F);
+
 /* Callback applying the remaining skeleton system: Y (n x nrhs, column-major, leading
  * dimension n, DEVICE memory) holds X(Si,:) of every instance in instance order; the
  * callback overwrites it with svfun(Y, trans) / mvfun(Y, trans) and returns 0, or returns

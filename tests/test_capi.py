@@ -81,3 +81,18 @@ def test_generators_match_oracle():
     Nb, ab, kb = configs.instance_batch(64, seed=3)
     np.testing.assert_array_equal(Na, Nb)
     np.testing.assert_array_equal(ka, kb)
+
+
+def test_factor_import_rejects_bad_factors():
+    good = dict(sk=np.array([0]), rd=np.array([1]), T=np.ones((1, 1)), L=np.ones((1, 1)), U=np.ones((1, 1)),
+                p=np.array([0]), E=np.ones((1, 1)), F=np.ones((1, 1)))
+    for bad, ident in [(dict(rd=np.array([5])), "FLAM:gpu:invalidFactor"),
+                       (dict(rd=np.array([0])), "FLAM:gpu:invalidFactor"),
+                       (dict(p=np.array([3])), "FLAM:gpu:invalidFactor")]:
+        f = dict(good, **bad)
+        with pytest.raises(fb.FlamError) as e:
+            fb.factor_import(dict(N=3, symm="n", factors=[f]))
+        assert e.value.identifier == ident
+    with pytest.raises(fb.FlamError) as e:
+        fb.factor_import(dict(N=3, symm="q", factors=[good]))
+    assert e.value.identifier == "FLAM:chksymm:invalidSymm"
