@@ -503,3 +503,84 @@ def rskelf_partial_mv(F, X, mvfun, trans="n"):
         X[F["Si"]] = mvfun(X[F["Si"]], t)
     X = _mv_half(F, X, t, False)
     return X[:, 0] if vec else X
+
+
+def rskelf_diag(F, dinv=0):
+    """D = rskelf_diag(F, dinv): diag(F) (dinv 0) or diag(inv(F)) (dinv 1) by unfolding the
+    factorization top-down on the sparse pattern of required entries.
+    rskelf/rskelf_diag.m:35-185 (symm n, s, p)."""
+    import scipy.sparse as sp
+    N, symm = F["N"], F["symm"]
+    lvp = np.asarray(F["lvp"])
+    nlvl = len(lvp) - 1
+    fs = F["factors"]
+    rem = np.ones(N, dtype=bool)
+    keep = [None] * max(nlvl, 1)
+    keep[0] = sp.csr_matrix((np.ones(N, dtype=bool), (np.arange(N), np.arange(N))), shape=(N, N))
+    for lvl in range(1, nlvl):                       # rskelf_diag.m:59-86
+        for f in fs[lvp[lvl - 1]:lvp[lvl]]:
+            rem[f["rd"]] = False
+        I_, J_ = keep[lvl - 1].nonzero()
+        m = rem[I_] & rem[J_]
+        Is, Js = [I_[m]], [J_[m]]
+        for f in fs[lvp[lvl - 1]:lvp[lvl]]:
+            a, b = np.meshgrid(f["sk"], f["sk"], indexing="ij")
+            Is.append(a.ravel())
+            Js.append(b.ravel())
+        I = np.concatenate(Is).astype(np.int64)
+        J = np.concatenate(Js).astype(np.int64)
+        if symm != "n":
+            m = I >= J
+            I, J = I[m], J[m]
+        keep[lvl] = sp.csr_matrix((np.ones(len(I), dtype=bool), (I, J)), shape=(N, N))
+        keep[lvl].sum_duplicates()
+        keep[lvl].data[:] = True
+    M = sp.csr_matrix((N, N))
+    for lvl in range(nlvl, 0, -1):                   # rskelf_diag.m:97-177
+        Ms = M.tocoo()
+        Is, Js, Vs = [Ms.row], [Ms.col], [Ms.data]
+        for f in fs[lvp[lvl - 1]:lvp[lvl]]:
+            sk, rd = f["sk"], f["rd"]
+            T, Lf, E = f["T"], f["L"], f["E"]
+            if symm in ("n", "s"):
+                U, G, p = f["U"], f["F"], f["p"]
+            else:
+                U, G, p = Lf.T, E.T, None
+            nrd, nsk = len(rd), len(sk)
+            ird = np.arange(nrd)
+            isk = nrd + np.arange(nsk)
+            X = np.zeros((nrd + nsk, nrd + nsk))
+            X[np.ix_(ird, ird)] = np.eye(nrd)
+            Xsk = M[sk][:, sk].toarray()
+            if symm != "n":                          # spsymm (core/spsymm.m): one of each pair stored
+                Xsk = Xsk + Xsk.T - np.diag(np.diag(Xsk))
+            X[np.ix_(isk, isk)] = Xsk
+            if dinv:
+                B = X[:, ird] - X[:, isk] @ E
+                X[:, ird] = sl.solve_triangular(Lf, B.T, trans="T", lower=True,
+                                                unit_diagonal=symm != "p").T
+                X[ird, :] = sl.solve_triangular(U, X[ird, :] - G @ X[isk, :], lower=False)
+                if p is not None:
+                    Xc = X[:, ird].copy()
+                    X[:, ird[p]] = Xc
+                X[:, isk] = X[:, isk] - X[:, ird] @ T.T
+                X[isk, :] = X[isk, :] - T @ X[ird, :]
+            else:
+                X[:, isk] = X[:, isk] + X[:, ird] @ G
+                X[isk, :] = X[isk, :] + E @ X[ird, :]
+                X[:, ird] = X[:, ird] @ U
+                X[ird, :] = Lf @ X[ird, :]
+                if p is not None:
+                    Xr = X[ird, :].copy()
+                    X[ird[p], :] = Xr
+                X[:, ird] = X[:, ird] + X[:, isk] @ T
+                X[ird, :] = X[ird, :] + T.T @ X[isk, :]
+            X[np.ix_(isk, isk)] -= Xsk
+            idx = np.concatenate([rd, sk])
+            a, b = np.meshgrid(idx, idx, indexing="ij")
+            Is.append(a.ravel())
+            Js.append(b.ravel())
+            Vs.append(X.ravel())
+        M = sp.csr_matrix((np.concatenate(Vs), (np.concatenate(Is), np.concatenate(Js))), shape=(N, N))
+        M = M.multiply(keep[lvl - 1]).tocsr()
+    return np.asarray(M.diagonal()).copy()

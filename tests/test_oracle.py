@@ -9,7 +9,7 @@ import pytest
 
 from oracle import configs
 from oracle.idecomp import id_
-from oracle.rskelf import (chksymm, chktrans, rskelf, rskelf_cholmv, rskelf_cholsv, rskelf_logdet, rskelf_mv,
+from oracle.rskelf import (chksymm, chktrans, rskelf, rskelf_cholmv, rskelf_cholsv, rskelf_diag, rskelf_logdet, rskelf_mv,
                            rskelf_partial_info, rskelf_partial_mv, rskelf_partial_sv, rskelf_sv)
 from oracle.snorm import snorm
 from oracle.tree import hypoct, hypoct_perm, mround, tree_arrays
@@ -209,6 +209,17 @@ def test_oracle_partial_sv_mv():
     assert np.linalg.norm(Ad @ X - B) / np.linalg.norm(B) < 1e-8
     Y = rskelf_partial_mv(F, B, lambda Z, t: (Ss if t == "n" else Ss.T) @ Z, "t")
     assert np.linalg.norm(Ad.T @ B - Y) / np.linalg.norm(Ad.T @ B) < 1e-8
+
+
+@pytest.mark.parametrize("symm", ["n", "s", "p"])
+def test_oracle_diag_matches_dense(symm):
+    # rskelf_diag.m: diag(F) and diag(inv(F)) by unfolding = the dense operator's diagonals
+    x, A, pxy = configs.star(600, seed=3, clustered=False) if symm == "n" else configs.circle(500)
+    F = rskelf(A, x, 32, 1e-10, pxy, dict(symm=symm))
+    N = x.shape[1]
+    Fd, Fi = rskelf_mv(F, np.eye(N)), rskelf_sv(F, np.eye(N))
+    assert np.abs(rskelf_diag(F, 0) - np.diag(Fd)).max() <= 1e-13 * np.abs(np.diag(Fd)).max()
+    assert np.abs(rskelf_diag(F, 1) - np.diag(Fi)).max() <= 1e-12 * np.abs(np.diag(Fi)).max()
 
 
 def test_rskelf_args():
