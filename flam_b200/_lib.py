@@ -23,7 +23,7 @@ EXPORTS = (
     "flam_factor_info", "flam_tree_export", "flam_tree_perm", "flam_factor_sizes", "flam_factor_export",
     "flam_level_stats", "flam_factor_free", "flam_workspace_release", "flam_profile", "flam_last_error", "flam_version",
     "flam_rskelf_cholmv", "flam_rskelf_cholsv", "flam_rskelf_logdet", "flam_partial_sizes", "flam_partial_export",
-    "flam_rskelf_partial_sv", "flam_rskelf_partial_mv", "flam_factor_import",
+    "flam_rskelf_partial_sv", "flam_rskelf_partial_mv", "flam_factor_import", "flam_rskelf_diag",
 )
 
 # int fn(double* Y, int64_t n, int64_t nrhs, char trans, void* stream, void* ctx)
@@ -107,6 +107,8 @@ def lib():
     L.flam_factor_import.argtypes = [C.c_int64, C.c_char, C.c_int64, i64p, i64p, i64p, i64p, dp, dp, dp, i64p, dp,
                                      dp, P, C.POINTER(P)]
     L.flam_factor_import.restype = C.c_int
+    L.flam_rskelf_diag.argtypes = [P, C.c_int, P]
+    L.flam_rskelf_diag.restype = C.c_int
     L.flam_rskelf_logdet.argtypes = [P, dp, dp]
     L.flam_rskelf_logdet.restype = C.c_int
     L.flam_partial_sizes.argtypes = [P, C.c_int, i64p, i64p]

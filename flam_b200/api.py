@@ -369,6 +369,21 @@ def rskelf_logdet(F):
     return out[0] if n == 1 else out
 
 
+def rskelf_diag(F, dinv=0):
+    """D = rskelf_diag(F, dinv): diag(F) (dinv 0) or diag(inv(F)) (dinv 1), N values
+    (all instances of a batched handle, in their concatenated order).
+    rskelf/rskelf_diag.m:35-185, computed by unfolding box by box on the device."""
+    D = np.zeros(F.info()["N"])
+    _lib.check(_lib.lib().flam_rskelf_diag(F.handle, int(bool(dinv)), C.c_void_p(D.ctypes.data)))
+    return D
+
+
+def rskelf_spdiag(F, dinv=0):
+    """D = rskelf_spdiag(F, dinv): the same diagonal as rskelf_diag (rskelf/rskelf_spdiag.m:19-85
+    reaches it by sparse applies on unit vectors; the device unfolding gives the same values)."""
+    return rskelf_diag(F, dinv)
+
+
 def rskelf_partial_info(F, inst=0):
     """[Si, S] = rskelf_partial_info(F)   rskelf/rskelf_partial_info.m:12-20 (S: scipy CSC)."""
     return F.partial_info(inst)

@@ -125,6 +125,15 @@ struct HostFac {
   int64_t fac_off, piv_off;
 };
 
+// A box of a factorization step, for the top-down unfolding of rskelf_diag: its
+// [sk rd] ids at ipool[slf_off, slf_off + n), k skeletons, and its factor (index
+// into hfac) or -1 when the box kept all its points (r = 0).
+struct BoxRec {
+  int64_t slf_off;
+  int32_t n, k;
+  int64_t fac;
+};
+
 // An M block left when an instance stops: rows/columns ipool[idx_off, idx_off + n),
 // values (column-major n x n) at val_off of the host copy.
 struct KeptBlock {
@@ -220,6 +229,7 @@ struct flam_factor {
   std::vector<std::vector<int64_t>> inst_fac;     // per instance: indices into hfac
   std::vector<std::vector<int64_t>> inst_lvp;     // per instance F.lvp
   std::vector<std::vector<LevelStat>> stats;
+  std::vector<std::vector<BoxRec>> step_boxes;    // per step, every box (rskelf_diag)
   std::vector<int64_t> rem;  // remaining points per instance
   // partial factorization (rskelf.m:278-308): per instance the remaining skeletons Si
   // (instance-local, ascending) and S in compressed-column form
@@ -1005,6 +1015,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // ---- elimination plan
     std::vector<ElimTask> et(nb);
     std::vector<FacDesc> fd;
+    std::vector<BoxRec> brec;
     int64_t mtop = 0;
     int kmx = 0, rmx = 0, nmax_e = 0;
     const bool chol = F.symm == 'p';
@@ -1040,6 +1051,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         f.r = r;
         fd.push_back(f);
         HostFac h{t.inst, step, slf_off[q], k, r, fpool_top, ppool_top};
+        brec.push_back(BoxRec{slf_off[q], n, k, (int64_t)F.hfac.size()});
         F.inst_fac[t.inst].push_back((int64_t)F.hfac.size());
         F.hfac.push_back(h);
         fpool_top += 2 * kr + rr + (chol ? 0 : kr);
@@ -1050,8 +1062,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       } else {
         t.fac_off = -1;
         t.piv_off = -1;
+        if (n > 0) brec.push_back(BoxRec{slf_off[q], n, k, -1});
       }
     }
+    F.step_boxes.push_back(std::move(brec));
     F.fpool.reserve(std::max<int64_t>(fpool_top, 1), s);
     F.fpool.n = fpool_top;
     F.ppool.reserve(std::max<int64_t>(ppool_top, 1), s);
@@ -1731,6 +1745,91 @@ flam_status flam_rskelf_logdet(const flam_factor* F, double* re, double* im) {
       if (re) re[i] = sr[i];
       if (im) im[i] = (par[i] & 1) ? pi : 0.0;   // mod(imag, 2*pi) of a multiple of pi
     }
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_rskelf_diag(const flam_factor* F, int dinv, double* D) {
+  return guard([&] {
+    if (!F || !D) fail(FLAM_ERR_ARG, "FLAM:rskelf_diag:invalidArg: NULL argument");
+    if (F->symm == 'h') fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h' is not built on the device");
+    if (F->step_boxes.size() != F->steps.size())
+      fail(FLAM_ERR_UNSUPPORTED, "FLAM:rskelf_diag:noTree: the handle has no box structure (imported factors)");
+    int64_t nrem = 0;
+    for (auto v : F->rem) nrem += v;
+    if (nrem > 0) fail(FLAM_ERR_ARG, "FLAM:rskelf_diag:partial: the factorization is partial (opts.stop)");
+    const cudaStream_t s = F->s;
+    const int64_t N = F->Ntot;
+    if (N == 0) return FLAM_OK;
+    const bool dev = is_device_ptr(D);
+    DBuf<double> xp[2], tmp, Dd;
+    DBuf<int64_t> xoff;
+    DBuf<int32_t> xpos, xld;
+    DBuf<UnfoldTask> tk;
+    xoff.resize(N, s);
+    xpos.resize(N, s);
+    xld.resize(N, s);
+    CK(cudaMemsetAsync(xoff.p, 0xff, sizeof(int64_t) * N, s));   // -1: no block yet
+    double* Dp = D;
+    if (!dev) {
+      Dd.resize(N, s);
+      Dp = Dd.p;
+    }
+    CK(cudaMemsetAsync(Dp, 0, sizeof(double) * N, s));
+    int cur = 0;
+    for (int q = (int)F->steps.size() - 1; q >= 0; --q) {   // top-down
+      const auto& br = F->step_boxes[q];
+      std::vector<UnfoldTask> ts;
+      int64_t xtop = 0, ttop = 0;
+      for (const BoxRec& b : br) {
+        UnfoldTask u{};
+        u.ids_off = b.slf_off;
+        u.n = b.n;
+        u.k = b.n;
+        u.fac_off = 0;
+        u.piv_off = 0;
+        if (b.fac >= 0) {
+          const HostFac& h = F->hfac[b.fac];
+          u.k = h.k;
+          u.fac_off = h.fac_off;
+          u.piv_off = h.piv_off;
+        }
+        u.xout = xtop;
+        u.tmp_off = ttop;
+        xtop += (int64_t)b.n * b.n;
+        ttop += (int64_t)b.n * (b.n - u.k);
+        ts.push_back(u);
+      }
+      if (ts.empty()) continue;
+      xp[cur].ensure(std::max<int64_t>(xtop, 1), s);
+      tmp.ensure(std::max<int64_t>(ttop, 1), s);
+      tk.upload(ts, s);
+      UnfoldArgs a{};
+      a.tasks = tk.p;
+      a.ipool = F->ipool.p;
+      a.fpool = F->fpool.p;
+      a.ppool = F->ppool.p;
+      a.xprev = xp[cur ^ 1].p ? xp[cur ^ 1].p : xp[cur].p;
+      a.xcur = xp[cur].p;
+      a.xoff = xoff.p;
+      a.xpos = xpos.p;
+      a.xld = xld.p;
+      a.tmp = tmp.p;
+      a.D = Dp;
+      a.dinv = dinv ? 1 : 0;
+      a.symm = F->symm;
+      launch_unfold(a, (int)ts.size(), s);
+      CK(cudaGetLastError());
+      F->prof.launches += 1;
+      cur ^= 1;
+    }
+    if (!dev) CK(cudaMemcpyAsync(D, Dp, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    for (auto* b : {&xp[0], &xp[1], &tmp, &Dd}) b->release(s);
+    xoff.release(s);
+    xpos.release(s);
+    xld.release(s);
+    tk.release(s);
+    CK(cudaStreamSynchronize(s));
     return FLAM_OK;
   });
 }

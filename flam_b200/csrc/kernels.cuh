@@ -93,6 +93,32 @@ void launch_from_pointmajor(const double* W, int64_t N, int nrhs, double* X, int
 // Rows idx (n of them) of the point-major W <-> column-major n x nrhs Y; dir 0 gathers, 1 scatters.
 void launch_rows_pm(double* W, int nrhs, const int64_t* idx, int64_t n, double* Y, int dir, cudaStream_t s);
 
+// Top-down unfolding for rskelf_diag (diag.cu): one task per box of a step.
+struct UnfoldTask {
+  int64_t ids_off;   // ipool offset of the box's [sk | rd] ids
+  int64_t fac_off;   // fpool offset of its factor [T | LU | E | G] (unused when r == 0)
+  int64_t piv_off;   // ppool offset of its LU permutation
+  int64_t xout;      // this box's n x n block in the current step's pool
+  int64_t tmp_off;   // n x r doubles of work space
+  int32_t n, k;
+};
+struct UnfoldArgs {
+  const UnfoldTask* tasks;
+  const int64_t* ipool;
+  const double* fpool;
+  const int32_t* ppool;
+  const double* xprev;  // blocks of the step above
+  double* xcur;         // blocks of this step
+  int64_t* xoff;        // per point: its block's offset (-1: none yet)
+  int32_t* xpos;        // per point: its row in that block
+  int32_t* xld;         // per point: that block's order
+  double* tmp;
+  double* D;            // per point: the diagonal
+  int dinv;
+  int symm;
+};
+void launch_unfold(const UnfoldArgs& a, int ntask, cudaStream_t s);
+
 // Per-factor log-determinant terms of one step: out[2f] = sum log|diag| (x2 if chol),
 // out[2f+1] = parity of (negative diagonal entries + inversions of p).
 void launch_logdet(const FacDesc* fac, int nfac, const double* fpool, const int32_t* ppool, int chol, double* out,

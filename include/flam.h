@@ -178,6 +178,14 @@ FLAM_API flam_status flam_rskelf_cholsv(const flam_factor* F, double* X, int64_t
  * for 'p'; sum log diag(U) + log detperm(p) for 'n'/'s'.  Either pointer may be NULL. */
 FLAM_API flam_status flam_rskelf_logdet(const flam_factor* F, double* re, double* im);
 
+/* D = rskelf_diag(F, dinv) / rskelf_spdiag(F, dinv): the diagonal of the factored
+ * matrix (dinv = 0) or of its inverse (dinv = 1), N values (all instances, host or device
+ * memory).  rskelf/rskelf_diag.m:35-185 (unfolding of the factorization top-down) and
+ * rskelf/rskelf_spdiag.m:19-85 compute the same D; this library unfolds box by box on the
+ * device.  symm 'n', 's', 'p'; a complete factorization made by flam_rskelf*
+ * (FLAM:rskelf_diag:partial for opts.stop, FLAM:rskelf_diag:noTree for imported factors). */
+FLAM_API flam_status flam_rskelf_diag(const flam_factor* F, int dinv, double* D);
+
 /* The remaining skeleton system of a partial factorization (opts.stop), per instance:
  * [Si, S] = rskelf_partial_info(F) -- rskelf/rskelf_partial_info.m:12-20, assembled as in
  * rskelf/rskelf.m:278-308.  The skeleton block left to the caller is A(Si,Si) + S.
