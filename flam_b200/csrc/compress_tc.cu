@@ -154,7 +154,8 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   __shared__ Stage<PH> st;
   __shared__ double vbuf[2][PH];
   __shared__ double tau2[2];
-  __shared__ AMx red_am[32];
+  __shared__ AMx red_am[2][32];
+  __shared__ double vcol[B == 16 ? 1024 : (B == 64 ? 256 : 512)];   // reflector of the pivoted QR step
   __shared__ double red_d[32];
   __shared__ int s_cnt[32];
   __shared__ int s_k, s_ktol, s_niter, s_cap, s_need;
@@ -306,12 +307,12 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
       AMx o2{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
       am = amx_better(am, o2);
     }
-    if (lane == 0) red_am[wid] = am;
+    AMx* ra = red_am[i & 1];   // alternating buffers: no barrier needed before the next step's writes
+    if (lane == 0) ra[wid] = am;
     __syncthreads();
-    AMx bm = red_am[0];
-    for (int w = 1; w < nw; ++w) bm = amx_better(bm, red_am[w]);
+    AMx bm = ra[0];
+    for (int w = 1; w < nw; ++w) bm = amx_better(bm, ra[w]);
     const int pvt = (bm.i >= i && bm.i < n) ? bm.i : i;   // NaN norms keep the column
-    __syncthreads();
     if (pvt != i) {
       for (int r = tid; r < n; r += NT) {
         const double tmp = R[(int64_t)r * ld + pvt];
@@ -327,10 +328,14 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
       }
     }
     __syncthreads();
-    if (wid == 0) {  // DLARFG on column i, rows i..m-1
+    if (wid == 0) {  // DLARFG on column i, rows i..m-1; the reflector is staged in shared memory
       double s = 0.0;
       if (i + 1 < m)
-        for (int r = i + 1 + lane; r < n; r += 32) s += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + i];
+        for (int r = i + 1 + lane; r < n; r += 32) {
+          const double v = R[(int64_t)r * ld + i];
+          vcol[r] = v;
+          s += v * v;
+        }
       s = warp_sum(s);
       double tau = 0.0;
       if (s != 0.0) {
@@ -338,7 +343,11 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         const double be = -copysign(hypot(al, sqrt(s)), al);
         tau = (be - al) / be;
         const double scal = 1.0 / (al - be);
-        for (int r = i + 1 + lane; r < n; r += 32) R[(int64_t)r * ld + i] *= scal;
+        for (int r = i + 1 + lane; r < n; r += 32) {
+          const double v = vcol[r] * scal;
+          vcol[r] = v;
+          R[(int64_t)r * ld + i] = v;
+        }
         __syncwarp();
         if (lane == 0) R[(int64_t)i * ld + i] = be;
       }
@@ -348,34 +357,31 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     const double tau = tau2[0];
     if (c > i && c < n) {
       if (tau != 0.0) {
-        // loads in groups of four so several are in flight (R may live in L2)
-        double w0 = R[(int64_t)i * ld + c], w1 = 0.0, w2 = 0.0, w3 = 0.0;
+        // column c from R (L2 for large n) eight rows at a time, the reflector from shared memory
+        double* Rc = R + c;
+        double w0 = Rc[(int64_t)i * ld], w1 = 0.0, w2 = 0.0, w3 = 0.0;
         int r = i + 1;
-        for (; r + 3 < n; r += 4) {
-          const double a0 = R[(int64_t)r * ld + i], a1 = R[(int64_t)(r + 1) * ld + i];
-          const double a2 = R[(int64_t)(r + 2) * ld + i], a3 = R[(int64_t)(r + 3) * ld + i];
-          const double b0 = R[(int64_t)r * ld + c], b1 = R[(int64_t)(r + 1) * ld + c];
-          const double b2 = R[(int64_t)(r + 2) * ld + c], b3 = R[(int64_t)(r + 3) * ld + c];
-          w0 += a0 * b0;
-          w1 += a1 * b1;
-          w2 += a2 * b2;
-          w3 += a3 * b3;
+        for (; r + 7 < n; r += 8) {
+          double b[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) b[u] = Rc[(int64_t)(r + u) * ld];
+          w0 += vcol[r] * b[0] + vcol[r + 4] * b[4];
+          w1 += vcol[r + 1] * b[1] + vcol[r + 5] * b[5];
+          w2 += vcol[r + 2] * b[2] + vcol[r + 6] * b[6];
+          w3 += vcol[r + 3] * b[3] + vcol[r + 7] * b[7];
         }
-        for (; r < n; ++r) w0 += R[(int64_t)r * ld + i] * R[(int64_t)r * ld + c];
+        for (; r < n; ++r) w0 += vcol[r] * Rc[(int64_t)r * ld];
         const double tw = tau * ((w0 + w1) + (w2 + w3));
-        R[(int64_t)i * ld + c] -= tw;
+        Rc[(int64_t)i * ld] -= tw;
         int rr = i + 1;
-        for (; rr + 3 < n; rr += 4) {
-          const double a0 = R[(int64_t)rr * ld + i], a1 = R[(int64_t)(rr + 1) * ld + i];
-          const double a2 = R[(int64_t)(rr + 2) * ld + i], a3 = R[(int64_t)(rr + 3) * ld + i];
-          const double b0 = R[(int64_t)rr * ld + c], b1 = R[(int64_t)(rr + 1) * ld + c];
-          const double b2 = R[(int64_t)(rr + 2) * ld + c], b3 = R[(int64_t)(rr + 3) * ld + c];
-          R[(int64_t)rr * ld + c] = b0 - tw * a0;
-          R[(int64_t)(rr + 1) * ld + c] = b1 - tw * a1;
-          R[(int64_t)(rr + 2) * ld + c] = b2 - tw * a2;
-          R[(int64_t)(rr + 3) * ld + c] = b3 - tw * a3;
+        for (; rr + 7 < n; rr += 8) {
+          double b[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) b[u] = Rc[(int64_t)(rr + u) * ld];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) Rc[(int64_t)(rr + u) * ld] = b[u] - tw * vcol[rr + u];
         }
-        for (; rr < n; ++rr) R[(int64_t)rr * ld + c] -= tw * R[(int64_t)rr * ld + i];
+        for (; rr < n; ++rr) Rc[(int64_t)rr * ld] -= tw * vcol[rr];
       }
       if (vn1[c] != 0.0) {  // partial norm downdate (xLAQP2)
         double temp = fabs(R[(int64_t)i * ld + c]) / vn1[c];
