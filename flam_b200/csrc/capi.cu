@@ -73,7 +73,7 @@ struct DBuf {
   int64_t n = 0, cap = 0;
   void reserve(int64_t c, cudaStream_t s) {
     if (c <= cap) return;
-    int64_t nc = std::max<int64_t>(c, cap + cap / 2);
+    int64_t nc = std::max<int64_t>(c, 2 * cap);
     nc = std::max<int64_t>(nc, 16);
     T* q = nullptr;
     CK(cudaMallocAsync(reinterpret_cast<void**>(&q), sizeof(T) * nc, s));
@@ -160,6 +160,11 @@ struct LevelStat {
 // one stream run in order, so they can share it; flam_workspace_release()
 // returns the memory.
 struct Workspace {
+  // final sizes of the last factorizations on this stream: a new factorization
+  // reserves its factor pools at these sizes once instead of growing them step by
+  // step (each growth is an allocation plus a copy; large stream-ordered
+  // allocations can cost the driver hundreds of ms when the pool is fragmented)
+  int64_t hint_ipool = 0, hint_fpool = 0, hint_ppool = 0;
   DBuf<int64_t> cpool;
   DBuf<double> tpool, scratch, mpool[2], W, tmp;
   DBuf<int32_t> permpool, status, mfilt;
@@ -751,6 +756,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   auto& cout = ws.cout;
   status.ensure(1, s);
   CK(cudaMemsetAsync(status.p, 0, sizeof(int32_t), s));
+  if (ws.hint_ipool > F.ipool.cap) F.ipool.reserve(ws.hint_ipool, s);
+  if (ws.hint_fpool > F.fpool.cap) F.fpool.reserve(ws.hint_fpool, s);
+  if (ws.hint_ppool > F.ppool.cap) F.ppool.reserve(ws.hint_ppool, s);
   Problem P;
   P.d = F.d;
   P.x = F.x.p;
@@ -1214,6 +1222,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   if (st & ST_NOT_SPD)
     fail(FLAM_ERR_NOT_SPD, "FLAM:rskelf:notPosDef: a redundant block is not positive definite (chol failed)");
   if (st & ST_SINGULAR) F.warn |= 2;
+  ws.hint_ipool = std::max(ws.hint_ipool, F.ipool.n);
+  ws.hint_fpool = std::max(ws.hint_fpool, F.fpool.n);
+  ws.hint_ppool = std::max(ws.hint_ppool, F.ppool.n);
   assemble_partial(F, kept, kept_val);
 }
 

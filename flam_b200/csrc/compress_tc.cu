@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   __shared__ double tau2[2];
   __shared__ AMx red_am[2][32];
   __shared__ double vcol[B == 16 ? 1024 : (B == 64 ? 256 : 512)];   // reflector of the pivoted QR step
-  __shared__ double red_d[32];
+  __shared__ double red_d[64];
   __shared__ int s_cnt[32];
   __shared__ int s_k, s_ktol, s_niter, s_cap, s_need;
 
@@ -313,48 +313,48 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     AMx bm = ra[0];
     for (int w = 1; w < nw; ++w) bm = amx_better(bm, ra[w]);
     const int pvt = (bm.i >= i && bm.i < n) ? bm.i : i;   // NaN norms keep the column
-    if (pvt != i) {
-      for (int r = tid; r < n; r += NT) {
-        const double tmp = R[(int64_t)r * ld + pvt];
+    // swap columns i and pvt, and gather column i's rows below the diagonal (the
+    // reflector) into shared memory with its sum of squares, one row per thread
+    double s = 0.0;
+    for (int r = tid; r < n; r += NT) {
+      double v = R[(int64_t)r * ld + pvt];
+      if (pvt != i) {
         R[(int64_t)r * ld + pvt] = R[(int64_t)r * ld + i];
-        R[(int64_t)r * ld + i] = tmp;
+        R[(int64_t)r * ld + i] = v;
       }
-      if (tid == 0) {
-        const int tj = jpvt[pvt];
-        jpvt[pvt] = jpvt[i];
-        jpvt[i] = tj;
-        vn1[pvt] = vn1[i];
-        vn2[pvt] = vn2[i];
+      if (r > i && i + 1 < m) {
+        vcol[r] = v;
+        s += v * v;
       }
     }
-    __syncthreads();
-    if (wid == 0) {  // DLARFG on column i, rows i..m-1; the reflector is staged in shared memory
-      double s = 0.0;
-      if (i + 1 < m)
-        for (int r = i + 1 + lane; r < n; r += 32) {
-          const double v = R[(int64_t)r * ld + i];
-          vcol[r] = v;
-          s += v * v;
-        }
-      s = warp_sum(s);
-      double tau = 0.0;
-      if (s != 0.0) {
-        const double al = R[(int64_t)i * ld + i];
-        const double be = -copysign(hypot(al, sqrt(s)), al);
-        tau = (be - al) / be;
-        const double scal = 1.0 / (al - be);
-        for (int r = i + 1 + lane; r < n; r += 32) {
-          const double v = vcol[r] * scal;
-          vcol[r] = v;
-          R[(int64_t)r * ld + i] = v;
-        }
-        __syncwarp();
-        if (lane == 0) R[(int64_t)i * ld + i] = be;
-      }
-      if (lane == 0) tau2[0] = tau;
+    if (tid == 0 && pvt != i) {
+      const int tj = jpvt[pvt];
+      jpvt[pvt] = jpvt[i];
+      jpvt[i] = tj;
+      vn1[pvt] = vn1[i];
+      vn2[pvt] = vn2[i];
     }
+    s = warp_sum(s);
+    double* rd_ = red_d + (i & 1) * 32;   // alternating halves
+    if (lane == 0) rd_[wid] = s;
     __syncthreads();
-    const double tau = tau2[0];
+    s = 0.0;
+    for (int w = 0; w < nw; ++w) s += rd_[w];
+    // DLARFG on column i, rows i..m-1, computed by every thread alike
+    double tau = 0.0, be = 0.0;
+    if (s != 0.0) {
+      const double al = R[(int64_t)i * ld + i];
+      be = -copysign(hypot(al, sqrt(s)), al);
+      tau = (be - al) / be;
+      const double scal = 1.0 / (al - be);
+      for (int r = i + 1 + tid; r < n; r += NT) {
+        const double v = vcol[r] * scal;
+        vcol[r] = v;
+        R[(int64_t)r * ld + i] = v;
+      }
+    }
+    __syncthreads();   // every thread has read R(i,i); the reflector is complete
+    if (tid == 0 && s != 0.0) R[(int64_t)i * ld + i] = be;
     if (c > i && c < n) {
       if (tau != 0.0) {
         // column c from R (L2 for large n) eight rows at a time, the reflector from shared memory
