@@ -1450,11 +1450,22 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
     CK(cudaEventCreate(&F->pend[1]));
     CK(cudaEventRecord(F->pend[0], s));
   }
+  // FLAM_PROFILE: one event pair per sweep launch, printed with the step's shape
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sev;
+  std::vector<int> sstep;
   auto sweep = [&](int q) {
     const StepDev& sd = F->steps[q];
     a.fac = sd.fac.p;
     if (sd.nfac == 0) return;
+    if (pp) {
+      sev.emplace_back();
+      CK(cudaEventCreate(&sev.back().first));
+      CK(cudaEventCreate(&sev.back().second));
+      CK(cudaEventRecord(sev.back().first, s));
+      sstep.push_back(q);
+    }
     launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
+    if (pp) CK(cudaEventRecord(sev.back().second, s));
     F->prof.launches += 1;
     F->prof.n_sweep += 1;
     F->prof.flop_sweep += sd.flop_per_rhs * (double)nrhs;
@@ -1510,6 +1521,15 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
             a[0], a[1], a[2], a[3], a[4], std::chrono::duration<double, std::milli>(henq - hstart).count(),
             std::chrono::duration<double, std::milli>(hend - henq).count());
     for (auto& e : pev) CK(cudaEventDestroy(e));
+    for (size_t e = 0; e < sev.size(); ++e) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, sev[e].first, sev[e].second));
+      const StepDev& sd = F->steps[sstep[e]];
+      fprintf(stderr, "[flam] sweep step %2d nfac %6d kmax %4d rmax %4d  %8.3f ms\n", sstep[e], sd.nfac, sd.kmax,
+              sd.rmax, ms);
+      CK(cudaEventDestroy(sev[e].first));
+      CK(cudaEventDestroy(sev[e].second));
+    }
   }
   return FLAM_OK;
 }

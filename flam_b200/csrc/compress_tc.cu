@@ -299,6 +299,13 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   }
   __syncthreads();
   const double tol3z = 1.0536712127723509e-08;  // sqrt(2^-53), LAPACK's dlamch('Epsilon')
+  // In tolerance mode the rank is the number of |R(i,i)| > tol |R(0,0)| (id.m:106-113);
+  // the pivoted diagonal does not increase, so the loop stops at the first entry at or
+  // below the tolerance: the skeleton set, R11 and R12 are final by then.  (Only the
+  // order of the redundant columns -- later pivots -- is left as it stands.)
+  const bool stop_early = a.kmax == 0 && !a.Aexp;
+  double r00 = 0.0;
+  int mn_eff = mn;
   for (int i = 0; i < mn; ++i) {
     AMx am{-1.0, n};
     if (c >= i && c < n) am = AMx{vn1[c], c};
@@ -342,9 +349,15 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     for (int w = 0; w < nw; ++w) s += rd_[w];
     // DLARFG on column i, rows i..m-1, computed by every thread alike
     double tau = 0.0, be = 0.0;
+    const double al = R[(int64_t)i * ld + i];
+    const double dii = s != 0.0 ? -copysign(hypot(al, sqrt(s)), al) : al;   // R(i,i) after this step
+    if (i == 0) r00 = fabs(dii);
+    if (stop_early && i > 0 && !(fabs(dii) > a.rel_tol * r00)) {
+      mn_eff = i;      // uniform: every thread computed the same dii
+      break;
+    }
     if (s != 0.0) {
-      const double al = R[(int64_t)i * ld + i];
-      be = -copysign(hypot(al, sqrt(s)), al);
+      be = dii;
       tau = (be - al) / be;
       const double scal = 1.0 / (al - be);
       for (int r = i + 1 + tid; r < n; r += NT) {
@@ -412,7 +425,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     const double tol = a.rel_tol * fabs(R[0]);
     int kt = 0;
     if (m > 0)
-      for (int i = 0; i < mn; ++i) kt += fabs(R[(int64_t)i * ld + i]) > tol;
+      for (int i = 0; i < mn_eff; ++i) kt += fabs(R[(int64_t)i * ld + i]) > tol;
     int kmax = a.kmax;
     if (kmax == 0 || kmax > n) kmax = n;
     s_ktol = kt;

@@ -147,13 +147,16 @@ __device__ void trmm(double* X, double* Y, Mat M, int r, bool lower, bool unit) 
 
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(SweepArgs a, double* gscr, int64_t slot) {
   extern __shared__ __align__(16) double smem[];
-  const FacDesc f = a.fac[blockIdx.x];
+  // consecutive CTAs take the right-hand-side tiles of one factor, so the factor's
+  // blocks are read from DRAM once and then from L2
+  const int ntile = (a.nrhs + kTs - 1) / kTs;
+  const FacDesc f = a.fac[blockIdx.x / ntile];
   const int k = f.k, r = f.r;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int c0 = blockIdx.y * kTs;
+  const int c0 = (blockIdx.x % ntile) * kTs;
   const int c = c0 + lane;
   const bool act = c < a.nrhs;
-  double* xs = gscr ? gscr + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * slot : smem;
+  double* xs = gscr ? gscr + (int64_t)blockIdx.x * slot : smem;
   double* xr = xs + (int64_t)k * kTs;
   double* yt = xr + (int64_t)r * kTs;   // scratch tile for the triangular products
   const int64_t* sk = a.ipool + f.sk_off;
@@ -331,21 +334,23 @@ void launch_rows_pm(double* W, int nrhs, const int64_t* idx, int64_t n, double* 
 
 void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t s) {
   if (nfac <= 0 || a.nrhs <= 0) return;
-  // X(sk), X(rd) and a scratch tile for the triangular products, kTs columns each
-  const int64_t slot = (int64_t)(kmax + 2 * rmax) * kTs;
+  // X(sk), X(rd) and, for the multiplies, a scratch tile for the triangular
+  // products (the solves work in place), kTs columns each
+  const int64_t slot = (int64_t)(kmax + (a.op >= 2 ? 2 : 1) * rmax) * kTs;
   const size_t need = sizeof(double) * (size_t)slot;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  dim3 g(nfac, (a.nrhs + kTs - 1) / kTs);
-  if (need <= 160 * 1024) {
+  const int64_t nblk = (int64_t)nfac * ((a.nrhs + kTs - 1) / kTs);
+  const unsigned g = (unsigned)nblk;
+  if (need <= 200 * 1024) {
     k_sweep<<<g, kSweepThreads, need, s>>>(a, nullptr, 0);
   } else {
     // rows of huge factors do not fit in shared memory: stage them in global scratch
     double* scr = nullptr;
-    cudaMallocAsync(&scr, sizeof(double) * slot * g.x * g.y, s);
+    cudaMallocAsync(&scr, sizeof(double) * slot * nblk, s);
     k_sweep<<<g, kSweepThreads, 0, s>>>(a, scr, slot);
     cudaFreeAsync(scr, s);
   }
