@@ -370,10 +370,23 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     if (tid == 0 && s != 0.0) R[(int64_t)i * ld + i] = be;
     if (c > i && c < n) {
       if (tau != 0.0) {
-        // column c from R (L2 for large n) eight rows at a time, the reflector from shared memory
+        // column c from R (L2 for large n) 32 rows at a time -- 32 loads in flight per
+        // thread hide the L2 latency of the long columns -- the reflector from shared memory
         double* Rc = R + c;
         double w0 = Rc[(int64_t)i * ld], w1 = 0.0, w2 = 0.0, w3 = 0.0;
         int r = i + 1;
+        for (; r + 31 < n; r += 32) {
+          double b[32];
+#pragma unroll
+          for (int u = 0; u < 32; ++u) b[u] = Rc[(int64_t)(r + u) * ld];
+#pragma unroll
+          for (int u = 0; u < 32; u += 4) {
+            w0 += vcol[r + u] * b[u];
+            w1 += vcol[r + u + 1] * b[u + 1];
+            w2 += vcol[r + u + 2] * b[u + 2];
+            w3 += vcol[r + u + 3] * b[u + 3];
+          }
+        }
         for (; r + 7 < n; r += 8) {
           double b[8];
 #pragma unroll
@@ -387,6 +400,13 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         const double tw = tau * ((w0 + w1) + (w2 + w3));
         Rc[(int64_t)i * ld] -= tw;
         int rr = i + 1;
+        for (; rr + 31 < n; rr += 32) {
+          double b[32];
+#pragma unroll
+          for (int u = 0; u < 32; ++u) b[u] = Rc[(int64_t)(rr + u) * ld];
+#pragma unroll
+          for (int u = 0; u < 32; ++u) Rc[(int64_t)(rr + u) * ld] = b[u] - tw * vcol[rr + u];
+        }
         for (; rr + 7 < n; rr += 8) {
           double b[8];
 #pragma unroll
