@@ -46,100 +46,112 @@ struct Mat {
   }
 };
 
-// Y(0:m, :) += sign * A(0:m, 0:q) X(0:q, :)
-__device__ void gemm_acc(double* Y, const double* X, Mat A, int m, int q, double sign) {
+// The factor blocks are read through 32 x 32 tiles staged in shared memory (At,
+// 32 x 33 doubles): every CTA thread loads a few entries with consecutive threads on
+// consecutive addresses, and the products then read the tile as warp broadcasts.
+constexpr int kAt = 33;   // row stride of the staged tile
+
+// At[ii][bb] = A(i0 + ii, b0 + bb) for ii < mi, bb < qb, masked to a triangle in
+// the (i, j) sense of A: tri 0 full, 1 lower (j <= i), 2 upper (j >= i); with unit the
+// diagonal reads 1.
+__device__ __forceinline__ void stage_tile(double* At, const Mat& A, int i0, int b0, int mi, int qb, int tri,
+                                           bool unit) {
+  const bool colmajor = A.rs == 1 && !A.rmap;
+  for (int e = threadIdx.x; e < 32 * 32; e += kSweepThreads) {
+    const int ii = colmajor ? (e & 31) : (e >> 5), bb = colmajor ? (e >> 5) : (e & 31);
+    double v = 0.0;
+    if (ii < mi && bb < qb) {
+      const int i = i0 + ii, j = b0 + bb;
+      const bool in = tri == 0 || (tri == 1 ? j <= i : j >= i);
+      if (in) v = (unit && i == j) ? 1.0 : A.at(i, j);
+    }
+    At[ii * kAt + bb] = v;
+  }
+}
+
+// Y(0:m, :) += sign * A(0:m, 0:q) X(0:q, :), A masked to a triangle by tri/unit as in
+// stage_tile.  Warp w owns rows w, w+8, w+16, w+24 of each 32-row block.  Y and X must
+// not overlap.  Called by every thread of the CTA.
+__device__ void gemm_acc(double* Y, const double* X, Mat A, int m, int q, double sign, double* At, int tri = 0,
+                         bool unit = false) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int i0 = w; i0 < m; i0 += 4 * kSw) {
+  for (int i0 = 0; i0 < m; i0 += 32) {
+    const int mi = min(32, m - i0);
+    int bs = 0, be = q;
+    if (tri == 1) be = min(q, i0 + 32);
+    if (tri == 2) bs = i0;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    const int i1 = i0 + kSw, i2 = i0 + 2 * kSw, i3 = i0 + 3 * kSw;
-    for (int b = 0; b < q; ++b) {
-      const double xb = X[b * kTs + lane];
-      s0 += A.at(i0, b) * xb;
-      if (i1 < m) s1 += A.at(i1, b) * xb;
-      if (i2 < m) s2 += A.at(i2, b) * xb;
-      if (i3 < m) s3 += A.at(i3, b) * xb;
+    for (int b0 = bs; b0 < be; b0 += 32) {
+      const int qb = min(32, q - b0);
+      __syncthreads();
+      stage_tile(At, A, i0, b0, mi, qb, tri, unit);
+      __syncthreads();
+      const double* a0 = At + w * kAt;
+#pragma unroll 8
+      for (int bb = 0; bb < qb; ++bb) {
+        const double xb = X[(b0 + bb) * kTs + lane];
+        s0 += a0[bb] * xb;
+        s1 += a0[8 * kAt + bb] * xb;
+        s2 += a0[16 * kAt + bb] * xb;
+        s3 += a0[24 * kAt + bb] * xb;
+      }
     }
-    Y[i0 * kTs + lane] += sign * s0;
-    if (i1 < m) Y[i1 * kTs + lane] += sign * s1;
-    if (i2 < m) Y[i2 * kTs + lane] += sign * s2;
-    if (i3 < m) Y[i3 * kTs + lane] += sign * s3;
+    if (w < mi) Y[(i0 + w) * kTs + lane] += sign * s0;
+    if (w + 8 < mi) Y[(i0 + w + 8) * kTs + lane] += sign * s1;
+    if (w + 16 < mi) Y[(i0 + w + 16) * kTs + lane] += sign * s2;
+    if (w + 24 < mi) Y[(i0 + w + 24) * kTs + lane] += sign * s3;
   }
 }
 
-// X = M^-1 X for M (r x r) lower triangular in the (i, j) sense of M.at: blocks of kSw rows,
-// the block's rows first take the contribution of the rows already solved (all warps),
-// then warp 0 solves the kSw x kSw diagonal block.
-__device__ void trsm_fwd(double* X, Mat M, int r, bool unit) {
+__device__ __forceinline__ Mat shift(const Mat& M, int i0, int j0) {
+  return Mat{M.p + i0 * M.rs + j0 * M.cs, M.rs, M.cs, nullptr, nullptr};
+}
+
+// X = M^-1 X for M (r x r) lower triangular in the (i, j) sense of M.at: 32-row blocks;
+// a block first takes the contribution of the rows already solved (gemm_acc), then
+// warp 0 solves the 32 x 32 diagonal block staged in shared memory.
+__device__ void trsm_fwd(double* X, Mat M, int r, bool unit, double* At) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int i0 = 0; i0 < r; i0 += kSw) {
-    const int i = i0 + w;
-    if (i < r && i0 > 0) {
-      double s0 = 0.0, s1 = 0.0;
-      int j = 0;
-      for (; j + 1 < i0; j += 2) {
-        s0 += M.at(i, j) * X[j * kTs + lane];
-        s1 += M.at(i, j + 1) * X[(j + 1) * kTs + lane];
-      }
-      if (j < i0) s0 += M.at(i, j) * X[j * kTs + lane];
-      X[i * kTs + lane] -= s0 + s1;
-    }
+  for (int i0 = 0; i0 < r; i0 += 32) {
+    const int ib = min(32, r - i0);
+    if (i0 > 0) gemm_acc(X + i0 * kTs, X, shift(M, i0, 0), ib, i0, -1.0, At);
     __syncthreads();
-    if (w == 0) {
-      const int i1 = min(i0 + kSw, r);
-      for (int ii = i0; ii < i1; ++ii) {
-        double v = X[ii * kTs + lane];
-        for (int jj = i0; jj < ii; ++jj) v -= M.at(ii, jj) * X[jj * kTs + lane];
-        X[ii * kTs + lane] = unit ? v : v / M.at(ii, ii);
+    stage_tile(At, M, i0, i0, ib, ib, 1, false);
+    __syncthreads();
+    if (w == 0)
+      for (int ii = 0; ii < ib; ++ii) {
+        double v = X[(i0 + ii) * kTs + lane];
+        for (int jj = 0; jj < ii; ++jj) v -= At[ii * kAt + jj] * X[(i0 + jj) * kTs + lane];
+        X[(i0 + ii) * kTs + lane] = unit ? v : v / At[ii * kAt + ii];
       }
-    }
     __syncthreads();
   }
 }
 
-// X = M^-1 X for M upper triangular (backward substitution), same blocking.
-__device__ void trsm_bwd(double* X, Mat M, int r, bool unit) {
+// X = M^-1 X for M upper triangular (backward substitution), 32-row blocks from the end.
+__device__ void trsm_bwd(double* X, Mat M, int r, bool unit, double* At) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int i1 = r; i1 > 0; i1 -= kSw) {
-    const int i0 = max(i1 - kSw, 0);
-    const int i = i0 + w;
-    if (i < i1 && i1 < r) {
-      double s0 = 0.0, s1 = 0.0;
-      int j = i1;
-      for (; j + 1 < r; j += 2) {
-        s0 += M.at(i, j) * X[j * kTs + lane];
-        s1 += M.at(i, j + 1) * X[(j + 1) * kTs + lane];
-      }
-      if (j < r) s0 += M.at(i, j) * X[j * kTs + lane];
-      X[i * kTs + lane] -= s0 + s1;
-    }
+  for (int i1 = r; i1 > 0; i1 -= 32) {
+    const int i0 = max(i1 - 32, 0), ib = i1 - i0;
+    if (i1 < r) gemm_acc(X + i0 * kTs, X + i1 * kTs, shift(M, i0, i1), ib, r - i1, -1.0, At);
     __syncthreads();
-    if (w == 0) {
-      for (int ii = i1 - 1; ii >= i0; --ii) {
-        double v = X[ii * kTs + lane];
-        for (int jj = ii + 1; jj < i1; ++jj) v -= M.at(ii, jj) * X[jj * kTs + lane];
-        X[ii * kTs + lane] = unit ? v : v / M.at(ii, ii);
+    stage_tile(At, M, i0, i0, ib, ib, 2, false);
+    __syncthreads();
+    if (w == 0)
+      for (int ii = ib - 1; ii >= 0; --ii) {
+        double v = X[(i0 + ii) * kTs + lane];
+        for (int jj = ii + 1; jj < ib; ++jj) v -= At[ii * kAt + jj] * X[(i0 + jj) * kTs + lane];
+        X[(i0 + ii) * kTs + lane] = unit ? v : v / At[ii * kAt + ii];
       }
-    }
     __syncthreads();
   }
 }
 
 // X = M X for M triangular (lower: j <= i, upper: j >= i) through the scratch tile Y.
-__device__ void trmm(double* X, double* Y, Mat M, int r, bool lower, bool unit) {
+__device__ void trmm(double* X, double* Y, Mat M, int r, bool lower, bool unit, double* At) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int i = w; i < r; i += kSw) {
-    const int j0 = lower ? 0 : i, j1 = lower ? i + 1 : r;
-    double s0 = 0.0, s1 = 0.0;
-    int j = j0;
-    for (; j + 1 < j1; j += 2) {
-      const double m0 = (unit && j == i) ? 1.0 : M.at(i, j);
-      const double m1 = (unit && j + 1 == i) ? 1.0 : M.at(i, j + 1);
-      s0 += m0 * X[j * kTs + lane];
-      s1 += m1 * X[(j + 1) * kTs + lane];
-    }
-    if (j < j1) s0 += ((unit && j == i) ? 1.0 : M.at(i, j)) * X[j * kTs + lane];
-    Y[i * kTs + lane] = s0 + s1;
-  }
+  for (int i = w; i < r; i += kSw) Y[i * kTs + lane] = 0.0;
+  gemm_acc(Y, X, M, r, r, 1.0, At, lower ? 1 : 2, unit);
   __syncthreads();
   for (int i = w; i < r; i += kSw) X[i * kTs + lane] = Y[i * kTs + lane];
   __syncthreads();
@@ -147,6 +159,7 @@ __device__ void trmm(double* X, double* Y, Mat M, int r, bool lower, bool unit) 
 
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(SweepArgs a, double* gscr, int64_t slot) {
   extern __shared__ __align__(16) double smem[];
+  __shared__ double At[32 * kAt];
   // consecutive CTAs take the right-hand-side tiles of one factor, so the factor's
   // blocks are read from DRAM once and then from L2
   const int ntile = (a.nrhs + kTs - 1) / kTs;
@@ -183,64 +196,64 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(SweepArgs a, double* gs
   const int tr = a.trans;
   switch (a.op) {
     case 0:  // sv upward
-      gemm_acc(xr, xs, gather_p ? Ttp : Tt, r, k, -1.0);
+      gemm_acc(xr, xs, gather_p ? Ttp : Tt, r, k, -1.0, At);
       __syncthreads();
       if (!lu) {
-        trsm_fwd(xr, Ln, r, false);
-        gemm_acc(xs, xr, En, k, r, -1.0);
+        trsm_fwd(xr, Ln, r, false, At);
+        gemm_acc(xs, xr, En, k, r, -1.0, At);
       } else if (!tr) {
-        trsm_fwd(xr, Ln, r, true);
-        gemm_acc(xs, xr, En, k, r, -1.0);
+        trsm_fwd(xr, Ln, r, true, At);
+        gemm_acc(xs, xr, En, k, r, -1.0, At);
       } else {
-        trsm_fwd(xr, Lt, r, false);      // U' \ x
-        gemm_acc(xs, xr, Gt, k, r, -1.0);
+        trsm_fwd(xr, Lt, r, false, At);      // U' \ x
+        gemm_acc(xs, xr, Gt, k, r, -1.0, At);
       }
       break;
     case 1:  // sv downward
       if (!lu) {
-        gemm_acc(xr, xs, Et, r, k, -1.0);
+        gemm_acc(xr, xs, Et, r, k, -1.0, At);
         __syncthreads();
-        trsm_bwd(xr, Lt, r, false);      // L' \ x
+        trsm_bwd(xr, Lt, r, false, At);      // L' \ x
       } else if (!tr) {
-        gemm_acc(xr, xs, Gn, r, k, -1.0);
+        gemm_acc(xr, xs, Gn, r, k, -1.0, At);
         __syncthreads();
-        trsm_bwd(xr, Ln, r, false);      // U \ x
+        trsm_bwd(xr, Ln, r, false, At);      // U \ x
       } else {
-        gemm_acc(xr, xs, Et, r, k, -1.0);
+        gemm_acc(xr, xs, Et, r, k, -1.0, At);
         __syncthreads();
-        trsm_bwd(xr, Lt, r, true);       // L' \ x, unit
+        trsm_bwd(xr, Lt, r, true, At);       // L' \ x, unit
       }
-      gemm_acc(xs, xr, scatter_p ? Tnp : Tn, k, r, -1.0);
+      gemm_acc(xs, xr, scatter_p ? Tnp : Tn, k, r, -1.0, At);
       break;
     case 2:  // mv upward
-      gemm_acc(xs, xr, gather_p ? Tnp : Tn, k, r, 1.0);
+      gemm_acc(xs, xr, gather_p ? Tnp : Tn, k, r, 1.0, At);
       __syncthreads();
       if (!lu) {
-        trmm(xr, yt, Lt, r, false, false);   // L' x
-        gemm_acc(xr, xs, Et, r, k, 1.0);
+        trmm(xr, yt, Lt, r, false, false, At);   // L' x
+        gemm_acc(xr, xs, Et, r, k, 1.0, At);
       } else if (!tr) {
-        trmm(xr, yt, Ln, r, false, false);   // U x
-        gemm_acc(xr, xs, Gn, r, k, 1.0);
+        trmm(xr, yt, Ln, r, false, false, At);   // U x
+        gemm_acc(xr, xs, Gn, r, k, 1.0, At);
       } else {
-        trmm(xr, yt, Lt, r, false, true);    // L' x, unit
-        gemm_acc(xr, xs, Et, r, k, 1.0);
+        trmm(xr, yt, Lt, r, false, true, At);    // L' x, unit
+        gemm_acc(xr, xs, Et, r, k, 1.0, At);
       }
       break;
     default:  // mv downward
       if (!lu) {
-        gemm_acc(xs, xr, En, k, r, 1.0);
+        gemm_acc(xs, xr, En, k, r, 1.0, At);
         __syncthreads();
-        trmm(xr, yt, Ln, r, true, false);    // L x
+        trmm(xr, yt, Ln, r, true, false, At);    // L x
       } else if (!tr) {
-        gemm_acc(xs, xr, En, k, r, 1.0);
+        gemm_acc(xs, xr, En, k, r, 1.0, At);
         __syncthreads();
-        trmm(xr, yt, Ln, r, true, true);     // L x, unit
+        trmm(xr, yt, Ln, r, true, true, At);     // L x, unit
       } else {
-        gemm_acc(xs, xr, Gt, k, r, 1.0);
+        gemm_acc(xs, xr, Gt, k, r, 1.0, At);
         __syncthreads();
-        trmm(xr, yt, Lt, r, true, false);    // U' x
+        trmm(xr, yt, Lt, r, true, false, At);    // U' x
       }
-      gemm_acc(xr, xs, scatter_p ? Ttp : Tt, r, k, 1.0);
+      gemm_acc(xr, xs, scatter_p ? Ttp : Tt, r, k, 1.0, At);
       break;
   }
   __syncthreads();
