@@ -65,6 +65,7 @@ struct MVal {
 
 __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
   extern __shared__ __align__(16) double smem[];
+  __shared__ __align__(16) double tsm[kTileSmemDoubles];
   __shared__ AM red[kWarps];
   __shared__ int s_piv;
   const ElimTask t = a.tasks[blockIdx.x];
@@ -103,37 +104,11 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
 
   const double* T = a.tpool + t.T_off;  // k x r, ld k
   if (k > 0) {
-    // K(rd,:) = K(rd,:) - T' K(sk,:)      (T.' for 's': identical for real data)
-    for (int col = tcol; col < n; col += kWarps) {
-      const double* Kc = K + (int64_t)col * n;
-      for (int i = tr; i < r; i += 32) {
-        const double* Ti = T + (int64_t)i * k;
-        double s0 = 0.0, s1 = 0.0;
-        int b = 0;
-        for (; b + 1 < k; b += 2) {
-          s0 += Ti[b] * Kc[b];
-          s1 += Ti[b + 1] * Kc[b + 1];
-        }
-        if (b < k) s0 += Ti[b] * Kc[b];
-        K[k + i + (int64_t)col * n] -= s0 + s1;
-      }
-    }
-    __syncthreads();
-    // K(:,rd) = K(:,rd) - K(:,sk) T
-    for (int j = tcol; j < r; j += kWarps) {
-      const double* Tj = T + (int64_t)j * k;
-      for (int row = tr; row < n; row += 32) {
-        double s0 = 0.0, s1 = 0.0;
-        int b = 0;
-        for (; b + 1 < k; b += 2) {
-          s0 += K[row + (int64_t)b * n] * Tj[b];
-          s1 += K[row + (int64_t)(b + 1) * n] * Tj[b + 1];
-        }
-        if (b < k) s0 += K[row + (int64_t)b * n] * Tj[b];
-        K[row + (int64_t)(k + j) * n] -= s0 + s1;
-      }
-    }
-    __syncthreads();
+    // K(rd,:) -= T' K(sk,:);  K(:,rd) -= K(:,sk) T   (T.' for 's': identical for real
+    // data), as 64 x 64 tiles with T staged through shared memory
+    const int64_t ldn = n;
+    cta_gemm(K + k, 1, ldn, GV{T, k, 1}, GV{K, 1, ldn}, r, n, k, -1.0, tsm);
+    cta_gemm(K + (int64_t)k * n, 1, ldn, GV{K, 1, ldn}, GV{T, 1, k}, n, r, k, -1.0, tsm);
   }
 
   double* Kr = K + k + (int64_t)k * n;  // r x r block, ld n
