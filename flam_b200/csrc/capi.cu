@@ -860,6 +860,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       const char* e = std::getenv("FLAM_SPLIT_MAX");
       return e ? std::max(1, std::atoi(e)) : 8;
     }();
+    static const int split_min_n = [] {  // boxes above this size are split (FLAM_SPLIT_MIN_N)
+      const char* e = std::getenv("FLAM_SPLIT_MIN_N");
+      return e ? std::max(1, std::atoi(e)) : 32;
+    }();
     int nparts = 1;
     while (nparts * 2 <= split_max && nparts * 2 * nb <= split_ctas) nparts *= 2;
     std::vector<char> split(nb, 0);
@@ -892,7 +896,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       const bool tc = n <= kTcMaxN;
       const int64_t mcap = (F.symm == 'n' ? 2 : 1) * ncand[q] +
                            (use_proxy ? (F.iph[i].two_sided ? 2 : 1) * (int64_t)F.npxy : 0);
-      split[q] = nparts > 1 && tc && n > 128 && mcap >= 64 * nparts;
+      split[q] = nparts > 1 && tc && n > split_min_n && mcap >= 64 * nparts;
       const bool c_glob = split[q] || (tc ? compress_tc_smem_bytes(n) > tc_smem_max() : n > kSmemN);
       const bool e_glob = n > kSmemN;
       t.scr_off = -1;
