@@ -483,10 +483,34 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     }
     __syncthreads();
     if (s_need) {
+      // the norms RRQR starts from, in parallel: r2(i) = |row i of inv(R11)|^2 by forward
+      // substitution on thread i (the row kept in column i of R's empty strict lower
+      // triangle), c2(j) = |column j of R22|^2 (id.m:120-121)
+      for (int i = tid; i < k; i += NT) {
+        const double yi = 1.0 / R[(int64_t)i * ld + i];
+        double s2 = yi * yi;
+        for (int j = i + 1; j < k; ++j) {
+          double sj = yi * R[(int64_t)i * ld + j];
+          for (int l = i + 1; l < j; ++l) sj += R[(int64_t)l * ld + i] * R[(int64_t)l * ld + j];
+          const double yj = -sj / R[(int64_t)j * ld + j];
+          R[(int64_t)j * ld + i] = yj;
+          s2 += yj * yj;
+        }
+        aux[i] = s2;
+      }
+      for (int j = tid; j < n - k; j += NT) {
+        double s2 = 0.0;
+        for (int row = k; row < ktol; ++row) s2 += R[(int64_t)row * ld + k + j] * R[(int64_t)row * ld + k + j];
+        aux[n + j] = s2;
+      }
+      __syncthreads();
+      for (int i = tid; i < k; i += NT)
+        for (int j = i + 1; j < k; ++j) R[(int64_t)j * ld + i] = 0.0;
+      __syncthreads();
       if (tid == 0) {
         int niter = 0, capped = 0;
         const double tol = a.rel_tol * fabs(R[0]);
-        const int kk = rrqr_serial(R, ld, 1, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped);
+        const int kk = rrqr_serial(R, ld, 1, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped, true);
         s_k = kk;
         s_niter = niter;
         s_cap = capped;

@@ -69,9 +69,11 @@ FLAM_HD inline void trisolve(const double* R, int64_t rs, int64_t cs, int k, con
 }
 
 // Sequential RRQR refinement of id.m:117-236 on thread 0.  R holds `rows` rows
-// (R11 | T) over n columns; returns the final rank, updates jpvt, niter.
+// (R11 | T) over n columns; returns the final rank, updates jpvt, niter.  With
+// norms_ready the caller has already put the squared row norms of inv(R11) in
+// aux[0:k] and the squared column norms of R22 in aux[n:2n-k] (id.m:120-121).
 FLAM_HD inline int rrqr_serial(double* R, int64_t rs, int64_t cs, int n, int k, int rows, int* jpvt, double tol, double Tmax,
-                           int64_t rrqr_iter, double* aux, int* niter_out, int* capped) {
+                           int64_t rrqr_iter, double* aux, int* niter_out, int* capped, bool norms_ready = false) {
   double* r2 = aux;            // k
   double* c2 = aux + n;        // n - k (+1)
   double* u = aux + 2 * n;     // k
@@ -79,16 +81,18 @@ FLAM_HD inline int rrqr_serial(double* R, int64_t rs, int64_t cs, int n, int k, 
   const double f2 = Tmax * Tmax;
   int niter = 0;
   // c2 = column norms^2 of R22, r2 = row norms^2 of inv(R11)
-  for (int j = 0; j < n - k; ++j) {
-    double s = 0.0;
-    for (int row = k; row < rows; ++row) s += R[(int64_t)(row) * rs + (int64_t)(k + j) * cs] * R[(int64_t)(row) * rs + (int64_t)(k + j) * cs];
-    c2[j] = s;
-  }
-  for (int i = 0; i < k; ++i) r2[i] = 0.0;
-  for (int j = 0; j < k; ++j) {
-    for (int i = 0; i < k; ++i) u[i] = (i == j) ? 1.0 : 0.0;
-    trisolve(R, rs, cs, k, u, 1, tv);
-    for (int i = 0; i < k; ++i) r2[i] += tv[i] * tv[i];
+  if (!norms_ready) {
+    for (int j = 0; j < n - k; ++j) {
+      double s = 0.0;
+      for (int row = k; row < rows; ++row) s += R[(int64_t)(row) * rs + (int64_t)(k + j) * cs] * R[(int64_t)(row) * rs + (int64_t)(k + j) * cs];
+      c2[j] = s;
+    }
+    for (int i = 0; i < k; ++i) r2[i] = 0.0;
+    for (int j = 0; j < k; ++j) {
+      for (int i = 0; i < k; ++i) u[i] = (i == j) ? 1.0 : 0.0;
+      trisolve(R, rs, cs, k, u, 1, tv);
+      for (int i = 0; i < k; ++i) r2[i] += tv[i] * tv[i];
+    }
   }
   bool conv = false;
   while ((rrqr_iter < 0 || niter < rrqr_iter) && niter < kRrqrCapH) {

@@ -230,7 +230,11 @@ def test_partial_batched_stacks_instances():
         Si, S = fb.rskelf_partial_info(F)
         Sib, Sb = Fb.partial_info(i)
         np.testing.assert_array_equal(Si, Sib)
-        np.testing.assert_array_equal(S.toarray(), Sb.toarray())
+        # a batch shares the levels with other instances, so the row-split form of the
+        # few-box levels can differ from the single run: S agrees to eps / tol
+        Sd, Sbd = S.toarray(), Sb.toarray()
+        np.testing.assert_array_equal(Sd != 0, Sbd != 0)
+        assert np.abs(Sd - Sbd).max() <= 1e-6 * np.abs(Sd).max()
         Ad = dense_of(x, A)
         blocks.append(Ad[np.ix_(Si, Si)] + S.toarray())
         off += x.shape[1]
