@@ -867,6 +867,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     int nparts = 1;
     while (nparts * 2 <= split_max && nparts * 2 * nb <= split_ctas) nparts *= 2;
     std::vector<char> split(nb, 0);
+    std::vector<int> npq(nb, 1);   // parts of each split box
     int64_t ttop = 0, ptop = 0, stop_s = 0;
     int nmax_small = 0;
     for (int q = 0; q < nb; ++q) {
@@ -896,13 +897,20 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       const bool tc = n <= kTcMaxN;
       const int64_t mcap = (F.symm == 'n' ? 2 : 1) * ncand[q] +
                            (use_proxy ? (F.iph[i].two_sided ? 2 : 1) * (int64_t)F.npxy : 0);
-      split[q] = nparts > 1 && tc && n > split_min_n && mcap >= 64 * nparts;
+      // as many parts (up to nparts) as leave each part at least one row panel
+      if (nparts > 1 && tc && n > split_min_n) {
+        const int64_t ph = (int64_t)compress_tc_rows(n) * compress_tc_group(n);
+        int np = nparts;
+        while (np > 1 && mcap < np * ph) np /= 2;
+        npq[q] = np;
+      }
+      split[q] = npq[q] > 1;
       const bool c_glob = split[q] || (tc ? compress_tc_smem_bytes(n) > tc_smem_max() : n > kSmemN);
       const bool e_glob = n > kSmemN;
       t.scr_off = -1;
       elim_scr[q] = -1;
       if (c_glob || e_glob) {
-        const int64_t cslot = split[q] ? nparts * compress_tc_doubles(n)
+        const int64_t cslot = split[q] ? npq[q] * compress_tc_doubles(n)
                                        : (tc ? compress_tc_doubles(n) : compress_scratch_doubles(n));
         const int64_t slot = std::max(cslot, elim_scratch_doubles(n));
         if (c_glob) t.scr_off = stop_s;
@@ -941,20 +949,20 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       for (int q : sord) cts.push_back(ct[q]);
       seg.push_back((int)cts.size());
       for (int q : sord)
-        for (int pt = 0; pt < nparts; ++pt) {
+        for (int pt = 0; pt < npq[q]; ++pt) {
           CompressTask u = ct[q];
           u.mode = 1;
           u.part = pt;
-          u.nparts = nparts;
+          u.nparts = npq[q];
           u.scr_off = ct[q].scr_off + pt * compress_tc_doubles(u.n);
           cts.push_back(u);
         }
       seg.push_back((int)cts.size());
-      for (int h = 1; h < nparts; h *= 2) {
+      for (int h = 1; h < nparts; h *= 2) {   // merge level h: boxes with more than h parts
         for (int q : sord)
-          for (int pt = 0; pt < nparts; pt += 2 * h) {
+          for (int pt = 0; pt + h < npq[q]; pt += 2 * h) {
             CompressTask u = ct[q];
-            u.mode = 2 * h == nparts ? 3 : 2;
+            u.mode = 2 * h == npq[q] ? 3 : 2;
             u.scr_off = ct[q].scr_off + pt * compress_tc_doubles(u.n);
             u.rsrc_off = ct[q].scr_off + (pt + h) * compress_tc_doubles(u.n);
             cts.push_back(u);
