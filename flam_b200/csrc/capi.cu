@@ -173,7 +173,13 @@ struct Workspace {
   DBuf<ChildBlock> chb;
   DBuf<CopySeg> segs, csegs;
   DBuf<CompressOut> cout;
+  cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
   void release(cudaStream_t s) {
+    if (copy) {
+      cudaStreamSynchronize(copy);
+      cudaStreamDestroy(copy);
+      copy = nullptr;
+    }
     for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp}) b->release(s);
     cpool.release(s);
     permpool.release(s);
@@ -1391,6 +1397,88 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
 // Which halves of the sweeps an apply runs.
 enum : int { kUp = 1, kDown = 2, kBoth = 3 };
 
+// The sweeps on a column-major device block Xd (N x nrhs, leading dimension ld), with the
+// point-major work array Wp (N x nrhs) -- launches only, on stream s.
+void sweeps_on_device(const flam_factor* F, double* Xd, int64_t ld, int64_t nrhs, double* Wp, int t, bool solve,
+                      int halves, cudaStream_t s) {
+  const int64_t N = F->Ntot;
+  launch_to_pointmajor(Xd, ld, N, (int)nrhs, Wp, s);
+  SweepArgs a{};
+  a.ipool = F->ipool.p;
+  a.fpool = F->fpool.p;
+  a.ppool = F->ppool.p;
+  a.X = Wp;
+  a.ldx = nrhs;
+  a.nrhs = (int)nrhs;
+  a.trans = t;
+  a.symm = F->symm;
+  const int ns = (int)F->steps.size();
+  auto sweep = [&](int q) {
+    const StepDev& sd = F->steps[q];
+    a.fac = sd.fac.p;
+    if (sd.nfac == 0) return;
+    launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
+    F->prof.launches += 1;
+    F->prof.n_sweep += 1;
+    F->prof.flop_sweep += sd.flop_per_rhs * (double)nrhs;
+    F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)nrhs;
+  };
+  F->prof.launches += 2;
+  if (halves & kUp) {
+    a.op = solve ? 0 : 2;
+    for (int q = 0; q < ns; ++q) sweep(q);
+  }
+  if (halves & kDown) {
+    a.op = solve ? 1 : 3;
+    for (int q = ns - 1; q >= 0; --q) sweep(q);
+  }
+  launch_from_pointmajor(Wp, N, (int)nrhs, Xd, ld, s);
+}
+
+// Apply with X in host memory: the right-hand sides go in two column halves whose
+// host->device copy, sweeps and device->host copy overlap (the copies run on the
+// workspace's copy stream, ordered by events).  Pinned X gives the overlap; pageable X
+// is still correct.
+flam_status apply_host_pipelined(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, int t, bool solve,
+                                 int halves) {
+  const cudaStream_t s = F->s;
+  const int64_t N = F->Ntot;
+  Workspace& ws = workspace(F->dev, s);
+  if (!ws.copy) CK(cudaStreamCreateWithFlags(&ws.copy, cudaStreamNonBlocking));
+  const cudaStream_t cs = ws.copy;
+  ws.tmp.ensure(N * nrhs, s);
+  ws.W.ensure(N * nrhs, s);
+  constexpr int kChunks = 2;
+  cudaEvent_t ev[2 * kChunks + 2];
+  for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  F->resolve_pending();
+  CK(cudaEventRecord(ev[0], s));     // the buffers are free once earlier work on s is done
+  CK(cudaStreamWaitEvent(cs, ev[0], 0));
+  int64_t c0[kChunks + 1];
+  for (int c = 0; c <= kChunks; ++c) c0[c] = nrhs * c / kChunks;
+  for (int c = 0; c < kChunks; ++c) {
+    const int64_t w = c0[c + 1] - c0[c];
+    CK(cudaMemcpy2DAsync(ws.tmp.p + N * c0[c], sizeof(double) * N, X + ldx * c0[c], sizeof(double) * ldx,
+                         sizeof(double) * N, w, cudaMemcpyHostToDevice, cs));
+    CK(cudaEventRecord(ev[1 + c], cs));
+  }
+  for (int c = 0; c < kChunks; ++c) {
+    const int64_t w = c0[c + 1] - c0[c];
+    CK(cudaStreamWaitEvent(s, ev[1 + c], 0));
+    sweeps_on_device(F, ws.tmp.p + N * c0[c], N, w, ws.W.p + N * c0[c], t, solve, halves, s);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ev[1 + kChunks + c], s));
+    CK(cudaStreamWaitEvent(cs, ev[1 + kChunks + c], 0));
+    CK(cudaMemcpy2DAsync(X + ldx * c0[c], sizeof(double) * ldx, ws.tmp.p + N * c0[c], sizeof(double) * N,
+                         sizeof(double) * N, w, cudaMemcpyDeviceToHost, cs));
+  }
+  CK(cudaEventRecord(ev[2 * kChunks + 1], cs));
+  CK(cudaStreamWaitEvent(s, ev[2 * kChunks + 1], 0));   // later work on s follows the copies
+  CK(cudaEventSynchronize(ev[2 * kChunks + 1]));
+  for (auto& e : ev) CK(cudaEventDestroy(e));
+  return FLAM_OK;
+}
+
 // The sweeps of rskelf_sv / rskelf_mv (solve = true / false) on X, in place.
 // halves selects the upward and/or downward half; with a skeleton function fn
 // (partial factorization) X(Si,:) is passed to fn between the halves
@@ -1417,6 +1505,7 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   const int t = (sweep_trans ? sweep_trans : tc) == 'n' ? 0 : 1;
   const int64_t N = F->Ntot;
   const bool dev = is_device_ptr(X);
+  if (!dev && !fn && !pp && nrhs >= 64) return apply_host_pipelined(F, X, ldx, nrhs, t, solve, halves);
   double* Xd = X;
   int64_t ld = ldx;
   Workspace& ws = workspace(F->dev, s);

@@ -320,3 +320,20 @@ def test_device_tensors():
     assert torch.equal(B, B0)                        # value semantics: the input is untouched
     X1 = fb.rskelf_sv(F1, np.asfortranarray(B.cpu().numpy()))
     np.testing.assert_array_equal(X2.cpu().numpy(), X1)
+
+
+def test_host_buffers_many_rhs_match_device():
+    # 64 or more right-hand sides in host memory go through the overlapped copy path
+    # (two column halves); every column is computed as on the device path
+    import torch
+    x, A, pxy = problems.star(5000, seed=4)
+    F = fb.rskelf(A, x, 64, 1e-10, pxy)
+    B = np.asfortranarray(np.random.default_rng(9).standard_normal((5000, 97)))
+    for fn, inplace in ((fb.rskelf_sv, F.sv_), (fb.rskelf_mv, F.mv_)):
+        Xh = fn(F, B)                                              # pageable host memory
+        P = torch.empty((97, 5000), dtype=torch.float64).pin_memory()
+        P.copy_(torch.from_numpy(B.T.copy()))
+        Xp = inplace(P.t().numpy())                                # pinned, in place
+        Xd = fn(F, torch.from_numpy(B.T.copy()).cuda().t()).cpu().numpy()
+        np.testing.assert_array_equal(Xh, Xd)
+        np.testing.assert_array_equal(Xp, Xd)
