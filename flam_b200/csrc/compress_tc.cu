@@ -595,8 +595,7 @@ void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, 
   if (b == 16)
     launch_b<16, 1>(a, ntask, nt, smem, s);
   else if (b == 64)
-    g == 4 ? launch_b<64, 4>(a, ntask, nt, smem, s)
-           : (g == 2 ? launch_b<64, 2>(a, ntask, nt, smem, s) : launch_b<64, 1>(a, ntask, nt, smem, s));
+    launch_b<64, 1>(a, ntask, nt, smem, s);   // 64-row panels are used with one thread per column
   else if (g == 4)
     launch_b<32, 4>(a, ntask, nt, smem, s);
   else if (g == 2)
