@@ -35,10 +35,10 @@ UNIT = "DOF/s"
 N_DEF, NRHS_DEF, OCC, TOL = 262144, 256, 64, 1e-10
 CPU_SAMPLE_N = 16384
 # DRAM bytes (read + write) per compress step of the N=262144 workload: one ncu capture
-# of every k_compress_tc launch of an N=65536 factorization (130.4 MB over its level
+# of every k_compress_tc launch of an N=65536 factorization (156.4 MB over its level
 # steps; profiles/k_compress_tc_star65536_top.md) scaled by the box count (x4) and
 # divided by this workload's 23 steps.
-COMPRESS_TRAFFIC_PER_STEP = 4 * 130.4e6 / 23
+COMPRESS_TRAFFIC_PER_STEP = 4 * 156.4e6 / 23
 
 
 def parse():
