@@ -174,11 +174,48 @@ struct Workspace {
   DBuf<CopySeg> segs, csegs;
   DBuf<CompressOut> cout;
   cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
+  // side streams for the independent launches of one step (the kernel shapes of a
+  // compress segment, the two elimination kernels): forked from the step's stream
+  // by one event and joined back by one event each
+  static constexpr int kSide = 6;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork = nullptr, join[kSide] = {};
+  void ensure_side() {
+    if (fork) return;
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (int i = 0; i < kSide; ++i) {
+      CK(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
+    }
+  }
+  // side streams 0..nuse-1 wait for the work issued on s so far
+  void fork_to(cudaStream_t s, int nuse) {
+    CK(cudaEventRecord(fork, s));
+    for (int i = 0; i < nuse; ++i) CK(cudaStreamWaitEvent(side[i], fork, 0));
+  }
+  // s waits for the work issued on side streams 0..nuse-1
+  void join_to(cudaStream_t s, int nuse) {
+    for (int i = 0; i < nuse; ++i) {
+      CK(cudaEventRecord(join[i], side[i]));
+      CK(cudaStreamWaitEvent(s, join[i], 0));
+    }
+  }
   void release(cudaStream_t s) {
     if (copy) {
       cudaStreamSynchronize(copy);
       cudaStreamDestroy(copy);
       copy = nullptr;
+    }
+    if (fork) {
+      for (int i = 0; i < kSide; ++i) {
+        cudaStreamSynchronize(side[i]);
+        cudaStreamDestroy(side[i]);
+        cudaEventDestroy(join[i]);
+        side[i] = nullptr;
+        join[i] = nullptr;
+      }
+      cudaEventDestroy(fork);
+      fork = nullptr;
     }
     for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp}) b->release(s);
     cpool.release(s);
@@ -748,6 +785,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   const int64_t stop = o.stop < 0 ? INT64_MAX : o.stop;
 
   Workspace& ws = workspace(F.dev, s);
+  ws.ensure_side();
   auto& cpool = ws.cpool;
   auto& tpool = ws.tpool;
   auto& scratch = ws.scratch;
@@ -778,6 +816,13 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   int64_t fpool_top = 0, ppool_top = 0;
   const bool prof = F.profile;
   const bool prof_print = std::getenv("FLAM_PROFILE") != nullptr;
+  // FLAM_PROFILE=2: also one event pair per compress launch, printed with its shape
+  const bool prof_launch = prof_print && std::getenv("FLAM_PROFILE")[0] == '2';
+  struct LaunchRec {
+    int key, t0, t1;
+    cudaEvent_t e0, e1;
+  };
+  std::vector<LaunchRec> lrec;
   // per-step CUDA events around the compress and elimination launches; resolved
   // after the last step so that profiling adds no synchronisation
   std::vector<cudaEvent_t> step_ev;
@@ -1005,25 +1050,44 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       pe = step_ev.data() + base;
       CK(cudaEventRecord(pe[0], s));
     }
-    // one launch per kernel shape within a segment of the task array
+    // one launch per kernel shape within a segment of the task array; the shapes
+    // (independent boxes) run concurrently on side streams, so that the few-box steps
+    // near the root, where every launch holds a few SMs, overlap their launches
     auto launch_segment = [&](int t0, int t1) {
+      std::vector<std::pair<int, int>> groups;
       for (int b0 = t0; b0 < t1;) {
         const int key = kkey_n(cts[b0].n);
         int b1 = b0;
-        size_t sm = 16;
-        while (b1 < t1 && kkey_n(cts[b1].n) == key) {
-          if (key > 0 && cts[b1].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(cts[b1].n));
-          ++b1;
-        }
-        CompressArgs cb = ca;
-        cb.tasks = ctask.p + b0;
-        if (key == 0)
-          launch_compress(cb, b1 - b0, compress_smem_bytes(nmax_small), s);
-        else
-          launch_compress_tc(cb, b1 - b0, key / 1000, (key / 10) % 100, key % 10, sm, s);
-        F.prof.launches += 1;
+        while (b1 < t1 && kkey_n(cts[b1].n) == key) ++b1;
+        groups.emplace_back(b0, b1);
         b0 = b1;
       }
+      const int nuse = std::min<int>((int)groups.size(), Workspace::kSide);
+      if (nuse > 1) ws.fork_to(s, nuse);
+      for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const int b0 = groups[gi].first, b1 = groups[gi].second;
+        const cudaStream_t gs = nuse > 1 ? ws.side[gi % Workspace::kSide] : s;
+        const int key = kkey_n(cts[b0].n);
+        size_t sm = 16;
+        for (int u = b0; u < b1; ++u)
+          if (key > 0 && cts[u].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(cts[u].n));
+        CompressArgs cb = ca;
+        cb.tasks = ctask.p + b0;
+        if (prof && prof_launch) {
+          LaunchRec lr{key, b0, b1, nullptr, nullptr};
+          CK(cudaEventCreate(&lr.e0));
+          CK(cudaEventCreate(&lr.e1));
+          CK(cudaEventRecord(lr.e0, gs));
+          lrec.push_back(lr);
+        }
+        if (key == 0)
+          launch_compress(cb, b1 - b0, compress_smem_bytes(nmax_small), gs);
+        else
+          launch_compress_tc(cb, b1 - b0, key / 1000, (key / 10) % 100, key % 10, sm, gs);
+        if (prof && prof_launch) CK(cudaEventRecord(lrec.back().e1, gs));
+        F.prof.launches += 1;
+      }
+      if (nuse > 1) ws.join_to(s, nuse);
     };
     launch_segment(0, seg[0]);
     if (seg.size() > 1) {
@@ -1135,7 +1199,16 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       }
     }
     if (prof) CK(cudaEventRecord(pe[2], s));
-    launch_eliminate(ea, nsmall_e, nb - nsmall_e, elim_smem_bytes(nmax_e), s);
+    if (nsmall_e > 0 && nb - nsmall_e > 0) {   // the two kernels' boxes are independent
+      ws.fork_to(s, 2);
+      launch_eliminate(ea, nsmall_e, 0, elim_smem_bytes(nmax_e), ws.side[0]);
+      ElimArgs eb = ea;
+      eb.tasks = etask.p + nsmall_e;
+      launch_eliminate(eb, 0, nb - nsmall_e, 0, ws.side[1]);
+      ws.join_to(s, 2);
+    } else {
+      launch_eliminate(ea, nsmall_e, nb - nsmall_e, elim_smem_bytes(nmax_e), s);
+    }
     CK(cudaGetLastError());
     if (prof) CK(cudaEventRecord(pe[3], s));
     if (prof && prof_print) {
@@ -1155,6 +1228,27 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       fprintf(stderr, "[flam] step %2d boxes %6d nmax %5lld big %4lld candmax %6lld mmax %6lld kmax %4lld rrqr %5lld"
               "  compress %8.3f ms  elim %8.3f ms\n", step, nb, (long long)nmx, (long long)nbig, (long long)cmx,
               (long long)mmx, (long long)kmx2, (long long)nit, tc, tel);
+      // per launch: tasks, sum of n, reflector steps of the row folding (panels x n)
+      for (LaunchRec& lr : lrec) {
+        float tl = 0;
+        CK(cudaEventElapsedTime(&tl, lr.e0, lr.e1));
+        const int ph = lr.key > 0 ? ((lr.key / 10) % 100) * (lr.key % 10) : 1;
+        int64_t sn = 0, nsteps = 0, nmx3 = 0, mode_mask = 0;
+        for (int u = lr.t0; u < lr.t1; ++u) {
+          const CompressTask& c = cts[u];
+          const int64_t mq = co[c.out_idx].m;
+          const int64_t rows = c.mode == 0 ? mq : (c.mode == 1 ? (mq * (c.part + 1)) / c.nparts - (mq * c.part) / c.nparts : c.n);
+          sn += c.n;
+          nmx3 = std::max<int64_t>(nmx3, c.n);
+          nsteps += (rows + ph - 1) / ph * c.n;
+          mode_mask |= 1 << c.mode;
+        }
+        fprintf(stderr, "[flam]   launch key %7d modes %lld tasks %6d sum_n %8lld nmax %5lld steps %10lld  %8.3f ms\n",
+                lr.key, (long long)mode_mask, lr.t1 - lr.t0, (long long)sn, (long long)nmx3, (long long)nsteps, tl);
+        CK(cudaEventDestroy(lr.e0));
+        CK(cudaEventDestroy(lr.e1));
+      }
+      lrec.clear();
     }
     StepDev sd;
     sd.fac.upload(fd, s);

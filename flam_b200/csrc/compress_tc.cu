@@ -55,7 +55,7 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 // Reflector j of the current panel, formed by the G threads that own column j
 // (thread g holds panel rows g*B .. g*B+B-1): annihilates the panel's column j
 // into R(j,j) (DLARFG conventions).
-template <int B, int G>
+template <int B, int G, int VS>
 __device__ __forceinline__ void reflect_col(double (&p)[B], double al, double* R, int ld, int j, int g,
                                             unsigned gmask, double* vb, double* tau_out) {
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;   // four chains: this sum is on the critical path
@@ -73,7 +73,7 @@ __device__ __forceinline__ void reflect_col(double (&p)[B], double al, double* R
     tau = (be - al) / be;
     const double scal = 1.0 / (al - be);
 #pragma unroll
-    for (int i = 0; i < B; ++i) vb[g * B + i] = p[i] * scal;
+    for (int i = 0; i < B; ++i) vb[g * VS + i] = p[i] * scal;
     __syncwarp(gmask);
     if (g == 0) R[(int64_t)j * ld + j] = be;
   }
@@ -150,9 +150,15 @@ __global__ void __launch_bounds__(256) k_filter(CompressArgs a) {
 template <int B, int G>
 __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_compress_tc(CompressArgs a) {
   constexpr int PH = B * G;  // panel height
+  // loads in flight per thread in the pivoted QR's column passes: 64 in the shape with
+  // the registers for them (64-row panels, 256 threads), else 32
+  constexpr int LD = B == 64 ? 64 : 32;
   extern __shared__ __align__(16) double smem[];
   __shared__ Stage<PH> st;
-  __shared__ double vbuf[2][PH];
+  // reflector of the row folding; lane g of a column reads its B entries at g * VS, so
+  // the G lanes of a column start on different banks
+  constexpr int VS = G == 1 ? B : B + 1;
+  __shared__ double vbuf[2][G * VS];
   __shared__ double tau2[2];
   __shared__ AMx red_am[2][32];
   __shared__ double vcol[B == 16 ? 1024 : (B == 64 ? 256 : 512)];   // reflector of the pivoted QR step
@@ -260,14 +266,14 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     // zero left of column p0: those reflectors are the identity and are skipped.
     const int js = Rsrc ? p0 : 0;
     double rcur = col < n ? R[(int64_t)js * ld + col] : 0.0;   // R(js, col)
-    if (col == js) reflect_col<B, G>(p, rcur, R, ld, js, g, gmask, vbuf[js & 1], &tau2[js & 1]);
+    if (col == js) reflect_col<B, G, VS>(p, rcur, R, ld, js, g, gmask, vbuf[js & 1], &tau2[js & 1]);
     __syncthreads();
     for (int j = js; j < n; ++j) {
       const int b = j & 1;
       const double rnext = (col > j && col < n && j + 1 < n) ? R[(int64_t)(j + 1) * ld + col] : 0.0;
       const double tau = tau2[b];
       if (tau != 0.0 && col > j && col < n) {
-        const double* v = vbuf[b] + g * B;
+        const double* v = vbuf[b] + g * VS;
         double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
 #pragma unroll
         for (int i = 0; i < B; i += 4) {
@@ -282,7 +288,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         for (int i = 0; i < B; ++i) p[i] -= tw * v[i];
       }
       if (col == j + 1 && col < n)
-        reflect_col<B, G>(p, rnext, R, ld, j + 1, g, gmask, vbuf[b ^ 1], &tau2[b ^ 1]);
+        reflect_col<B, G, VS>(p, rnext, R, ld, j + 1, g, gmask, vbuf[b ^ 1], &tau2[b ^ 1]);
       rcur = rnext;
       __syncthreads();
     }
@@ -370,17 +376,17 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     if (tid == 0 && s != 0.0) R[(int64_t)i * ld + i] = be;
     if (c > i && c < n) {
       if (tau != 0.0) {
-        // column c from R (L2 for large n) 32 rows at a time -- 32 loads in flight per
+        // column c from R (L2 for large n) LD rows at a time -- LD loads in flight per
         // thread hide the L2 latency of the long columns -- the reflector from shared memory
         double* Rc = R + c;
         double w0 = Rc[(int64_t)i * ld], w1 = 0.0, w2 = 0.0, w3 = 0.0;
         int r = i + 1;
-        for (; r + 31 < n; r += 32) {
-          double b[32];
+        for (; r + LD - 1 < n; r += LD) {
+          double b[LD];
 #pragma unroll
-          for (int u = 0; u < 32; ++u) b[u] = Rc[(int64_t)(r + u) * ld];
+          for (int u = 0; u < LD; ++u) b[u] = Rc[(int64_t)(r + u) * ld];
 #pragma unroll
-          for (int u = 0; u < 32; u += 4) {
+          for (int u = 0; u < LD; u += 4) {
             w0 += vcol[r + u] * b[u];
             w1 += vcol[r + u + 1] * b[u + 1];
             w2 += vcol[r + u + 2] * b[u + 2];
@@ -400,12 +406,12 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         const double tw = tau * ((w0 + w1) + (w2 + w3));
         Rc[(int64_t)i * ld] -= tw;
         int rr = i + 1;
-        for (; rr + 31 < n; rr += 32) {
-          double b[32];
+        for (; rr + LD - 1 < n; rr += LD) {
+          double b[LD];
 #pragma unroll
-          for (int u = 0; u < 32; ++u) b[u] = Rc[(int64_t)(rr + u) * ld];
+          for (int u = 0; u < LD; ++u) b[u] = Rc[(int64_t)(rr + u) * ld];
 #pragma unroll
-          for (int u = 0; u < 32; ++u) Rc[(int64_t)(rr + u) * ld] = b[u] - tw * vcol[rr + u];
+          for (int u = 0; u < LD; ++u) Rc[(int64_t)(rr + u) * ld] = b[u] - tw * vcol[rr + u];
         }
         for (; rr + 7 < n; rr += 8) {
           double b[8];
