@@ -180,6 +180,14 @@ struct Workspace {
   static constexpr int kSide = 6;
   cudaStream_t side[kSide] = {};
   cudaEvent_t fork = nullptr, join[kSide] = {};
+  // The elimination of a step runs on its own two streams (boxes with n <= 128 and
+  // larger ones) while the host plans the next step and its compress runs: the
+  // T / permutation / scratch pools alternate between two sets by step parity, and
+  // edone[parity][stream] marks the end of that step's elimination kernels.
+  DBuf<double> tpool_b, scratch_b;
+  DBuf<int32_t> permpool_b;
+  cudaStream_t es[2] = {};
+  cudaEvent_t ecomp = nullptr, eprep = nullptr, edone[2][2] = {};
   void ensure_side() {
     if (fork) return;
     CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -187,6 +195,17 @@ struct Workspace {
       CK(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
     }
+    CK(cudaEventCreateWithFlags(&ecomp, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&eprep, cudaEventDisableTiming));
+    for (int i = 0; i < 2; ++i) {
+      CK(cudaStreamCreateWithFlags(&es[i], cudaStreamNonBlocking));
+      for (int j = 0; j < 2; ++j) CK(cudaEventCreateWithFlags(&edone[i][j], cudaEventDisableTiming));
+    }
+  }
+  // s waits for the elimination kernels of the steps with parity par
+  void wait_elim(cudaStream_t s, int par) {
+    CK(cudaStreamWaitEvent(s, edone[par][0], 0));
+    CK(cudaStreamWaitEvent(s, edone[par][1], 0));
   }
   // side streams 0..nuse-1 wait for the work issued on s so far
   void fork_to(cudaStream_t s, int nuse) {
@@ -216,7 +235,22 @@ struct Workspace {
       }
       cudaEventDestroy(fork);
       fork = nullptr;
+      for (int i = 0; i < 2; ++i) {
+        cudaStreamSynchronize(es[i]);
+        cudaStreamDestroy(es[i]);
+        es[i] = nullptr;
+        for (int j = 0; j < 2; ++j) {
+          cudaEventDestroy(edone[i][j]);
+          edone[i][j] = nullptr;
+        }
+      }
+      cudaEventDestroy(ecomp);
+      cudaEventDestroy(eprep);
+      ecomp = eprep = nullptr;
     }
+    tpool_b.release(s);
+    scratch_b.release(s);
+    permpool_b.release(s);
     for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp}) b->release(s);
     cpool.release(s);
     permpool.release(s);
@@ -787,10 +821,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   Workspace& ws = workspace(F.dev, s);
   ws.ensure_side();
   auto& cpool = ws.cpool;
-  auto& tpool = ws.tpool;
-  auto& scratch = ws.scratch;
   auto& mpool = ws.mpool;
-  auto& permpool = ws.permpool;
   auto& status = ws.status;
   auto& ctask = ws.ctask;
   auto& etask = ws.etask;
@@ -833,6 +864,13 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   const int64_t nrun = std::min<int64_t>(stop, maxsteps);
 
   for (int step = 0; step < maxsteps && step < stop; ++step) {
+    // this step's T / permutation / scratch set was last read by the elimination two
+    // steps back
+    const int par = step & 1;
+    auto& tpool = par ? ws.tpool_b : ws.tpool;
+    auto& scratch = par ? ws.scratch_b : ws.scratch;
+    auto& permpool = par ? ws.permpool_b : ws.permpool;
+    ws.wait_elim(s, par);
     // ---- boxes of this step: level nlvl_i - step of each instance
     std::vector<int32_t> boxes;
     std::vector<int> binst_step;
@@ -870,6 +908,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       nslf[q] = n;
       top += n;
     }
+    if (top > F.ipool.cap) ws.wait_elim(s, par ^ 1);   // growth frees the pool the last elimination reads
     F.ipool.reserve(top, s);
     F.ipool.n = top;
     // ---- neighbour candidates: current xi of every neighbour (rskelf.m:186)
@@ -1156,11 +1195,17 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       }
     }
     F.step_boxes.push_back(std::move(brec));
-    F.fpool.reserve(std::max<int64_t>(fpool_top, 1), s);
+    // the elimination's pools grow, and its tasks upload, on its first stream, after
+    // this step's compress and the previous step's elimination
+    const cudaStream_t es0 = ws.es[0], es1 = ws.es[1];
+    CK(cudaEventRecord(ws.ecomp, s));
+    CK(cudaStreamWaitEvent(es0, ws.ecomp, 0));
+    CK(cudaStreamWaitEvent(es0, ws.edone[par ^ 1][1], 0));
+    F.fpool.reserve(std::max<int64_t>(fpool_top, 1), es0);
     F.fpool.n = fpool_top;
-    F.ppool.reserve(std::max<int64_t>(ppool_top, 1), s);
+    F.ppool.reserve(std::max<int64_t>(ppool_top, 1), es0);
     F.ppool.n = ppool_top;
-    mpool[cur].ensure(std::max<int64_t>(mtop, 1), s);
+    mpool[cur].ensure(std::max<int64_t>(mtop, 1), es0);
     // boxes whose work matrix is in global memory go to the blocked kernel: upload them last
     std::vector<ElimTask> ets;
     ets.reserve(nb);
@@ -1169,8 +1214,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     const int nsmall_e = (int)ets.size();
     for (const ElimTask& e : et)
       if (e.n > kSmemN) ets.push_back(e);
-    etask.upload(ets, s);
-    chb.upload(ch, s);
+    etask.upload(ets, es0);
+    chb.upload(ch, es0);
     ElimArgs ea{};
     ea.P = P;
     ea.tasks = etask.p;
@@ -1198,19 +1243,22 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         F.prof.flop_elim += 4 * k * r * n + fac + 2 * k * k * r;
       }
     }
-    if (prof) CK(cudaEventRecord(pe[2], s));
-    if (nsmall_e > 0 && nb - nsmall_e > 0) {   // the two kernels' boxes are independent
-      ws.fork_to(s, 2);
-      launch_eliminate(ea, nsmall_e, 0, elim_smem_bytes(nmax_e), ws.side[0]);
+    if (prof) CK(cudaEventRecord(pe[2], es0));
+    CK(cudaEventRecord(ws.eprep, es0));
+    if (nsmall_e > 0) launch_eliminate(ea, nsmall_e, 0, elim_smem_bytes(nmax_e), es0);
+    if (nb - nsmall_e > 0) {   // the two kernels' boxes are independent
+      CK(cudaStreamWaitEvent(es1, ws.eprep, 0));
       ElimArgs eb = ea;
       eb.tasks = etask.p + nsmall_e;
-      launch_eliminate(eb, 0, nb - nsmall_e, 0, ws.side[1]);
-      ws.join_to(s, 2);
-    } else {
-      launch_eliminate(ea, nsmall_e, nb - nsmall_e, elim_smem_bytes(nmax_e), s);
+      launch_eliminate(eb, 0, nb - nsmall_e, 0, es1);
     }
     CK(cudaGetLastError());
-    if (prof) CK(cudaEventRecord(pe[3], s));
+    CK(cudaEventRecord(ws.edone[par][0], es0));
+    CK(cudaEventRecord(ws.edone[par][1], es1));
+    if (prof) {
+      CK(cudaStreamWaitEvent(es0, ws.edone[par][1], 0));
+      CK(cudaEventRecord(pe[3], es0));
+    }
     if (prof && prof_print) {
       CK(cudaEventSynchronize(pe[3]));
       float tc = 0, tel = 0;
@@ -1275,6 +1323,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     {
       const bool last = step + 1 == nrun;
       std::vector<double> mh;
+      if (last) ws.wait_elim(s, par);
       if (last && mtop > 0) mh = download(mpool[cur].p, mtop, s);
       for (int q = 0; q < nb; ++q) {
         const int32_t b = boxes[q];
@@ -1286,6 +1335,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         if (last) {
           std::copy(mh.begin() + Moff[b], mh.begin() + Moff[b] + nn, kept_val.end() - nn);
         } else {
+          ws.wait_elim(s, par);
           auto v = download(mpool[cur].p + Moff[b], nn, s);
           std::copy(v.begin(), v.end(), kept_val.end() - nn);
         }
@@ -1303,6 +1353,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     }
     cur ^= 1;
   }
+  ws.wait_elim(s, 0);
+  ws.wait_elim(s, 1);
   // make sure the pools reflect their sizes
   int32_t st = 0;
   CK(cudaMemcpyAsync(&st, status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
