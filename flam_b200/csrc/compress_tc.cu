@@ -150,9 +150,9 @@ __global__ void __launch_bounds__(256) k_filter(CompressArgs a) {
 template <int B, int G>
 __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_compress_tc(CompressArgs a) {
   constexpr int PH = B * G;  // panel height
-  // loads in flight per thread in the pivoted QR's column passes: 64 in the shape with
-  // the registers for them (64-row panels, 256 threads), else 32
-  constexpr int LD = B == 64 ? 64 : 32;
+  // loads in flight per thread in the pivoted QR's column passes (64 measured slower in
+  // the 64-row shape: it spills at 255 registers)
+  constexpr int LD = 32;
   extern __shared__ __align__(16) double smem[];
   __shared__ Stage<PH> st;
   // reflector of the row folding; lane g of a column reads its B entries at g * VS, so
