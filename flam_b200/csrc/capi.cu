@@ -1250,6 +1250,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       CK(cudaStreamWaitEvent(es1, ws.eprep, 0));
       ElimArgs eb = ea;
       eb.tasks = etask.p + nsmall_e;
+      int rbig = 0;   // the largest redundant block among the big boxes: its LU panel height
+      for (int q = nsmall_e; q < nb; ++q) rbig = std::max(rbig, ets[q].n - ets[q].k);
+      eb.pan_rows = rbig <= elim_pan_rows_max() ? rbig : 0;
       launch_eliminate(eb, 0, nb - nsmall_e, 0, es1);
     }
     CK(cudaGetLastError());

@@ -11,6 +11,8 @@
 // local permutation.  LU is right-looking with partial pivoting (the first
 // maximum of |column|, as xGETF2), swapping whole rows so that the sk columns
 // end up as K(rd(p),sk).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "tile_f64.cuh"
@@ -252,6 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_eliminate(ElimArgs a) {
 constexpr int kNb = 32;
 
 __global__ void __launch_bounds__(kThreads) k_eliminate_big(ElimArgs a) {
+  extern __shared__ __align__(16) double pan[];   // LU panel: a.pan_rows x kNb doubles
   __shared__ __align__(16) double tsm[kTileSmemDoubles];
   __shared__ double blk[kNb * (kNb + 1)];
   __shared__ AM red[kWarps];
@@ -319,43 +322,93 @@ __global__ void __launch_bounds__(kThreads) k_eliminate_big(ElimArgs a) {
       cta_gemm(&kr(j1, j1), 1, ldn, GV{&kr(j1, j0), 1, ldn}, GV{&kr(j1, j0), ldn, 1}, r - j1, r - j1, jb, -1.0,
                tsm, 1);
     } else {
-      for (int j = j0; j < j1; ++j) {
-        AM am{-1.0, r};
-        for (int q = j + tid; q < r; q += kThreads) am = amax(am, AM{fabs(kr(q, j)), q});
+      if (r <= a.pan_rows) {
+        // the panel (rows j0.., jb columns) in shared memory: its pivot searches, swaps,
+        // scalings and rank-1 updates read no L2
+        const int pr = r - j0;
+        auto pp = [&](int i, int c) -> double& { return pan[(i - j0) + c * pr]; };
+        for (int e = tid; e < pr * jb; e += kThreads) pan[e] = kr(j0 + e % pr, j0 + e / pr);
+        __syncthreads();
+        for (int j = j0; j < j1; ++j) {
+          const int jl = j - j0;
+          AM am{-1.0, r};
+          for (int q = j + tid; q < r; q += kThreads) am = amax(am, AM{fabs(pp(q, jl)), q});
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          AM b{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
-          am = amax(am, b);
+          for (int o = 16; o > 0; o >>= 1) {
+            AM b{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+            am = amax(am, b);
+          }
+          if (lane == 0) red[wid] = am;
+          __syncthreads();
+          if (tid == 0) {
+            AM bm = red[0];
+            for (int w = 1; w < kWarps; ++w) bm = amax(bm, red[w]);
+            const int pv0 = (bm.i >= j && bm.i < r) ? bm.i : j;
+            s_piv = pv0;
+            piv[j] = pv0;
+          }
+          __syncthreads();
+          const int pv = (s_piv >= j && s_piv < r) ? s_piv : j;
+          if (pv != j && tid < jb) {
+            const double x = pp(j, tid);
+            pp(j, tid) = pp(pv, tid);
+            pp(pv, tid) = x;
+          }
+          __syncthreads();
+          const double dj = pp(j, jl);
+          if (dj != 0.0) {
+            for (int q = j + 1 + tid; q < r; q += kThreads) pp(q, jl) /= dj;
+          } else if (tid == 0) {
+            atomicOr(a.status, (int)ST_SINGULAR);
+          }
+          __syncthreads();
+          for (int c = jl + 1 + tcol; c < jb; c += kWarps) {
+            const double ujc = pp(j, c);
+            for (int q = j + 1 + tr; q < r; q += 32) pp(q, c) -= pp(q, jl) * ujc;
+          }
+          __syncthreads();
         }
-        if (lane == 0) red[wid] = am;
+        for (int e = tid; e < pr * jb; e += kThreads) kr(j0 + e % pr, j0 + e / pr) = pan[e];
         __syncthreads();
-        if (tid == 0) {
-          AM bm = red[0];
-          for (int w = 1; w < kWarps; ++w) bm = amax(bm, red[w]);
-          const int pv0 = (bm.i >= j && bm.i < r) ? bm.i : j;
-          s_piv = pv0;
-          piv[j] = pv0;
+      } else {
+        for (int j = j0; j < j1; ++j) {
+          AM am{-1.0, r};
+          for (int q = j + tid; q < r; q += kThreads) am = amax(am, AM{fabs(kr(q, j)), q});
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            AM b{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+            am = amax(am, b);
+          }
+          if (lane == 0) red[wid] = am;
+          __syncthreads();
+          if (tid == 0) {
+            AM bm = red[0];
+            for (int w = 1; w < kWarps; ++w) bm = amax(bm, red[w]);
+            const int pv0 = (bm.i >= j && bm.i < r) ? bm.i : j;
+            s_piv = pv0;
+            piv[j] = pv0;
+          }
+          __syncthreads();
+          const int pv = (s_piv >= j && s_piv < r) ? s_piv : j;
+          if (pv != j && tid < jb) {  // inside the panel; the other columns after it
+            const double x = kr(j, j0 + tid);
+            kr(j, j0 + tid) = kr(pv, j0 + tid);
+            kr(pv, j0 + tid) = x;
+          }
+          __syncthreads();
+          const double dj = kr(j, j);
+          if (dj != 0.0) {
+            for (int q = j + 1 + tid; q < r; q += kThreads) kr(q, j) /= dj;
+          } else if (tid == 0) {
+            atomicOr(a.status, (int)ST_SINGULAR);
+          }
+          __syncthreads();
+          for (int c = j + 1 + tcol; c < j1; c += kWarps) {
+            const double ujc = kr(j, c);
+            for (int q = j + 1 + tr; q < r; q += 32) kr(q, c) -= kr(q, j) * ujc;
+          }
+          __syncthreads();
         }
-        __syncthreads();
-        const int pv = (s_piv >= j && s_piv < r) ? s_piv : j;
-        if (pv != j && tid < jb) {  // inside the panel; the other columns after it
-          const double x = kr(j, j0 + tid);
-          kr(j, j0 + tid) = kr(pv, j0 + tid);
-          kr(pv, j0 + tid) = x;
-        }
-        __syncthreads();
-        const double dj = kr(j, j);
-        if (dj != 0.0) {
-          for (int q = j + 1 + tid; q < r; q += kThreads) kr(q, j) /= dj;
-        } else if (tid == 0) {
-          atomicOr(a.status, (int)ST_SINGULAR);
-        }
-        __syncthreads();
-        for (int c = j + 1 + tcol; c < j1; c += kWarps) {
-          const double ujc = kr(j, c);
-          for (int q = j + 1 + tr; q < r; q += 32) kr(q, c) -= kr(q, j) * ujc;
-        }
-        __syncthreads();
       }
       // the panel's interchanges on every other column of K (whole rows of K(rd,:))
       for (int col = tid; col < n; col += kThreads) {
@@ -510,14 +563,21 @@ void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cuda
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_eliminate, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_eliminate_big, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
   if (nsmall > 0) k_eliminate<<<nsmall, kThreads, smem, s>>>(a);
   if (nbig > 0) {
     ElimArgs b = a;
     b.tasks = a.tasks + nsmall;
-    k_eliminate_big<<<nbig, kThreads, 0, s>>>(b);
+    b.pan_rows = std::min(std::max(b.pan_rows, 0), elim_pan_rows_max());
+    k_eliminate_big<<<nbig, kThreads, sizeof(double) * (size_t)b.pan_rows * kNb, s>>>(b);
   }
 }
+
+// Rows of the largest LU panel k_eliminate_big stages in shared memory (200 KB of kNb
+// columns); the kernel holds all 65,536 registers of an SM, so the shared memory costs no
+// occupancy.
+int elim_pan_rows_max() { return (200 * 1024) / (int)(sizeof(double) * kNb); }
 
 }  // namespace flam

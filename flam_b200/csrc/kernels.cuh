@@ -58,9 +58,11 @@ struct ElimArgs {
   double* scratch;      // work matrices of boxes with n > kSmemN
   int32_t* status;      // OR of StatusBits
   int symm;             // 'n', 's', 'p', 'h'
+  int pan_rows;         // big boxes: rows of the LU panel staged in shared memory (0: none)
 };
 
 size_t elim_smem_bytes(int n);
+int elim_pan_rows_max();
 int64_t elim_scratch_doubles(int n);
 // tasks[0, nsmall): n <= kSmemN (shared-memory kernel); tasks[nsmall, nsmall + nbig): the rest.
 void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cudaStream_t s);
