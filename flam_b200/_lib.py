@@ -14,7 +14,7 @@ FLAM_OK = 0
 STATUS = {
     0: "FLAM_OK", 1: "FLAM_ERR_ARG", 2: "FLAM_ERR_NOT_SPD", 3: "FLAM_ERR_CUDA", 4: "FLAM_ERR_NOMEM",
     5: "FLAM_ERR_UNSUPPORTED", 6: "FLAM_ERR_TIMEOUT", 7: "FLAM_ERR_ID_CHECK",
-    100: "FLAM_WARN_RRQR_MAXITER", 101: "FLAM_WARN_SINGULAR",
+    100: "FLAM_WARN_RRQR_MAXITER", 101: "FLAM_WARN_SINGULAR", 102: "FLAM_WARN_IR_NOT_CONVERGED",
 }
 
 # every symbol include/flam.h declares
@@ -24,6 +24,7 @@ EXPORTS = (
     "flam_level_stats", "flam_factor_free", "flam_workspace_release", "flam_profile", "flam_last_error", "flam_version",
     "flam_rskelf_cholmv", "flam_rskelf_cholsv", "flam_rskelf_logdet", "flam_partial_sizes", "flam_partial_export",
     "flam_rskelf_partial_sv", "flam_rskelf_partial_mv", "flam_factor_import", "flam_rskelf_diag",
+    "flam_matvec", "flam_rskelf_ir_sv",
 )
 
 # int fn(double* Y, int64_t n, int64_t nrhs, char trans, void* stream, void* ctx)
@@ -107,6 +108,11 @@ def lib():
     L.flam_factor_import.argtypes = [C.c_int64, C.c_char, C.c_int64, i64p, i64p, i64p, i64p, dp, dp, dp, i64p, dp,
                                      dp, P, C.POINTER(P)]
     L.flam_factor_import.restype = C.c_int
+    L.flam_matvec.argtypes = [P, P, C.c_int64, C.c_int64, P, C.c_int64, P, C.c_int64]
+    L.flam_matvec.restype = C.c_int
+    L.flam_rskelf_ir_sv.argtypes = [P, P, C.c_int64, P, C.c_int64, C.c_int64, C.c_double, C.c_int,
+                                    C.POINTER(C.c_int), dp]
+    L.flam_rskelf_ir_sv.restype = C.c_int
     L.flam_rskelf_diag.argtypes = [P, C.c_int, P]
     L.flam_rskelf_diag.restype = C.c_int
     L.flam_rskelf_logdet.argtypes = [P, dp, dp]

@@ -222,6 +222,48 @@ class Factor:
         _lib.check(fn(self._h, C.c_void_p(X.ctypes.data), X.shape[0], nrhs, str(trans).encode()[:1], *extra))
         return X
 
+    # ------------------------------------------------------- FP64 products and refinement
+    @staticmethod
+    def _block(X, name):
+        """(pointer, leading dimension, columns) of a float64 column-major CUDA tensor or NumPy array."""
+        if _is_cuda_tensor(X):
+            import torch
+            if X.dtype != torch.float64:
+                raise _lib.FlamError(1, f"FLAM:{name}:invalidArg: arrays must be float64")
+            if X.dim() == 1:
+                return X.data_ptr(), X.shape[0], 1
+            if X.stride(0) != 1:
+                raise _lib.FlamError(1, f"FLAM:{name}:invalidArg: arrays must be column-major")
+            return X.data_ptr(), X.stride(1), X.shape[1]
+        if not (isinstance(X, np.ndarray) and X.dtype == np.float64 and (X.ndim == 1 or X.flags.f_contiguous)):
+            raise _lib.FlamError(1, f"FLAM:{name}:invalidArg: arrays must be float64 Fortran-ordered")
+        return X.ctypes.data, X.shape[0], 1 if X.ndim == 1 else X.shape[1]
+
+    def matvec_(self, X, Y, B=None):
+        """Y = A X (or B - A X) with the handle's registry matrix in FP64 (flam_matvec)."""
+        px, lx, nrhs = self._block(X, "matvec")
+        py, ly, ny = self._block(Y, "matvec")
+        pb, lb = (None, 1) if B is None else self._block(B, "matvec")[:2]
+        if ny != nrhs:
+            raise _lib.FlamError(1, "FLAM:matvec:invalidArg: X and Y need the same number of columns")
+        _lib.check(_lib.lib().flam_matvec(self._h, C.c_void_p(px), lx, nrhs, None if pb is None else C.c_void_p(pb),
+                                          lb, C.c_void_p(py), ly))
+        return Y
+
+    def ir_sv_(self, B, X, ir_tol=1e-10, max_iter=10):
+        """X = A \\ B by FP64 iterative refinement on this factorization (flam_rskelf_ir_sv).
+        Returns (X, refinement steps, per-column FP64 relative residuals)."""
+        pb, lb, nrhs = self._block(B, "rskelf_ir_sv")
+        px, lx, nx = self._block(X, "rskelf_ir_sv")
+        if nx != nrhs:
+            raise _lib.FlamError(1, "FLAM:rskelf_ir_sv:invalidArg: B and X need the same number of columns")
+        it = C.c_int()
+        rel = np.zeros(max(nrhs, 1))
+        _lib.check(_lib.lib().flam_rskelf_ir_sv(self._h, C.c_void_p(pb), lb, C.c_void_p(px), lx, nrhs, float(ir_tol),
+                                                int(max_iter), C.byref(it),
+                                                rel.ctypes.data_as(C.POINTER(C.c_double))))
+        return X, it.value, rel[:nrhs]
+
     # ------------------------------------------------------- partial factorization
     def partial_info(self, inst=0):
         """[Si, S] = rskelf_partial_info(F): remaining skeletons (0-based, ascending) and the
@@ -344,6 +386,17 @@ def rskelf_sv(F, X, trans="n"):
 def rskelf_mv(F, X, trans="n"):
     """Y = rskelf_mv(F, X, trans): returns a new array."""
     return F.mv_(_fresh_copy(X), trans)
+
+
+def matvec(F, X):
+    """Y = A X with the FP64 registry matrix of F (an O(N^2) product evaluated on the fly)."""
+    return F.matvec_(X, _fresh_copy(X))
+
+
+def rskelf_ir_sv(F, B, ir_tol=1e-10, max_iter=10):
+    """X = A \\ B by iterative refinement with F as the approximate inverse and the FP64
+    residual B - A X.  Returns (X, refinement steps, per-column relative residuals)."""
+    return F.ir_sv_(B, _fresh_copy(B), ir_tol, max_iter)
 
 
 def rskelf_cholmv(F, X, trans="n"):

@@ -26,6 +26,7 @@
 #include "../../include/flam.h"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "matvec.cuh"
 #include "scan.cuh"
 #include "tree.cuh"
 
@@ -173,6 +174,9 @@ struct Workspace {
   DBuf<ChildBlock> chb;
   DBuf<CopySeg> segs, csegs;
   DBuf<CompressOut> cout;
+  // FP64 products with the registry matrix and iterative refinement (matvec.cu)
+  DBuf<MatvecTile> mvt;
+  DBuf<double> irB, irX, irR, irW, colsq;
   cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
   // side streams for the independent launches of one step (the kernel shapes of a
   // compress segment, the two elimination kernels): forked from the step's stream
@@ -251,7 +255,8 @@ struct Workspace {
     tpool_b.release(s);
     scratch_b.release(s);
     permpool_b.release(s);
-    for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp}) b->release(s);
+    for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp, &irB, &irX, &irR, &irW, &colsq}) b->release(s);
+    mvt.release(s);
     cpool.release(s);
     permpool.release(s);
     status.release(s);
@@ -777,6 +782,20 @@ void assemble_partial(flam_factor& F, const std::vector<KeptBlock>& kept, const 
   }
 }
 
+// Device view of a handle's matrix and proxy.
+Problem problem_of(const flam_factor& F) {
+  Problem P;
+  P.d = F.d;
+  P.x = F.x.p;
+  P.w = F.has_w ? F.w.p : nullptr;
+  P.nrm = F.has_nrm ? F.nrm.p : nullptr;
+  P.ip = F.ip.p;
+  P.pxy_pts = F.pxy_pts.p;
+  P.pxy_shift = F.pxy_shift.n ? F.pxy_shift.p : nullptr;
+  P.npxy = F.npxy;
+  return P;
+}
+
 void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   cudaStream_t s = F.s;
   const int ninst = F.ninst;
@@ -834,15 +853,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   if (ws.hint_ipool > F.ipool.cap) F.ipool.reserve(ws.hint_ipool, s);
   if (ws.hint_fpool > F.fpool.cap) F.fpool.reserve(ws.hint_fpool, s);
   if (ws.hint_ppool > F.ppool.cap) F.ppool.reserve(ws.hint_ppool, s);
-  Problem P;
-  P.d = F.d;
-  P.x = F.x.p;
-  P.w = F.has_w ? F.w.p : nullptr;
-  P.nrm = F.has_nrm ? F.nrm.p : nullptr;
-  P.ip = F.ip.p;
-  P.pxy_pts = F.pxy_pts.p;
-  P.pxy_shift = F.pxy_shift.n ? F.pxy_shift.p : nullptr;
-  P.npxy = F.npxy;
+  const Problem P = problem_of(F);
   int cur = 0;  // M pool written this step
   int64_t fpool_top = 0, ppool_top = 0;
   const bool prof = F.profile;
@@ -1784,6 +1795,154 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   return FLAM_OK;
 }
 
+// ---------------------------------------------------------------- FP64 products (K10)
+// Yd = A Xd, or Yd = Bd - A Xd, on device blocks (column-major), launches only.
+void matvec_device(const flam_factor* F, const double* Xd, int64_t ldx, int64_t nrhs, const double* Bd, int64_t ldb,
+                   double* Yd, int64_t ldy, cudaStream_t s) {
+  Workspace& ws = workspace(F->dev, s);
+  const int tm = matvec_tile_rows((int)nrhs);
+  std::vector<MatvecTile> tiles;
+  for (int i = 0; i < F->ninst; ++i)
+    for (int64_t r = F->inst_off[i]; r < F->inst_off[i + 1]; r += tm)
+      tiles.push_back(MatvecTile{r, (int32_t)std::min<int64_t>(tm, F->inst_off[i + 1] - r), i});
+  ws.mvt.upload(tiles, s);
+  MatvecArgs a{};
+  a.P = problem_of(*F);
+  a.tiles = ws.mvt.p;
+  a.X = Xd;
+  a.ldx = ldx;
+  a.B = Bd;
+  a.ldb = ldb;
+  a.Y = Yd;
+  a.ldy = ldy;
+  a.nrhs = (int)nrhs;
+  launch_matvec(a, (int)tiles.size(), s);
+  F->prof.launches += 1;
+}
+
+void check_matrix(const flam_factor* F) {
+  if (!F) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: NULL factor");
+  if (!F->x.p || !F->ip.p)
+    fail(FLAM_ERR_ARG, "FLAM:gpu:noMatrix: the handle holds no registry matrix (imported factors)");
+}
+
+// A block on the device: the caller's pointer if it is device memory, else a copy in buf.
+const double* device_block(const double* X, int64_t ldx, int64_t N, int64_t nrhs, DBuf<double>& buf, int64_t* ld,
+                           cudaStream_t s) {
+  if (is_device_ptr(X)) {
+    *ld = ldx;
+    return X;
+  }
+  buf.ensure(N * nrhs, s);
+  CK(cudaMemcpy2DAsync(buf.p, sizeof(double) * N, X, sizeof(double) * ldx, sizeof(double) * N, nrhs,
+                       cudaMemcpyHostToDevice, s));
+  *ld = N;
+  return buf.p;
+}
+
+flam_status matvec(const flam_factor* F, const double* X, int64_t ldx, int64_t nrhs, const double* B, int64_t ldb,
+                   double* Y, int64_t ldy) {
+  check_matrix(F);
+  const int64_t N = F->Ntot;
+  if (nrhs < 0 || ldx < N || ldy < N || (B && ldb < N)) fail(FLAM_ERR_ARG, "FLAM:matvec:invalidArg: bad dimensions");
+  if (nrhs == 0) return FLAM_OK;
+  if (!X || !Y) fail(FLAM_ERR_ARG, "FLAM:matvec:invalidArg: X and Y must not be NULL");
+  const cudaStream_t s = F->s;
+  Workspace& ws = workspace(F->dev, s);
+  int64_t lx = 0, lb = 0;
+  const double* Xd = device_block(X, ldx, N, nrhs, ws.irX, &lx, s);
+  const double* Bd = B ? device_block(B, ldb, N, nrhs, ws.irB, &lb, s) : nullptr;
+  const bool ydev = is_device_ptr(Y);
+  double* Yd = Y;
+  int64_t ly = ldy;
+  if (!ydev) {
+    ws.irR.ensure(N * nrhs, s);
+    Yd = ws.irR.p;
+    ly = N;
+  }
+  matvec_device(F, Xd, lx, nrhs, Bd, lb, Yd, ly, s);
+  CK(cudaGetLastError());
+  if (!ydev) {
+    CK(cudaMemcpy2DAsync(Y, sizeof(double) * ldy, Yd, sizeof(double) * N, sizeof(double) * N, nrhs,
+                         cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  return FLAM_OK;
+}
+
+// X = A \ B by iterative refinement on the handle's factorization: X = F \ B, then while
+// max_j ||B_j - A X_j|| / ||B_j|| > tol: X += F \ (B - A X), with the FP64 residual of
+// matvec_device.  The factorization may be loose (a larger rank_or_tol) or mixed precision;
+// the residual, and so the reported error, is FP64.
+flam_status ir_solve(const flam_factor* F, const double* B, int64_t ldb, double* X, int64_t ldx, int64_t nrhs,
+                     double tol, int maxit, int* iters, double* relres) {
+  check_matrix(F);
+  const int64_t N = F->Ntot;
+  if (nrhs < 0 || ldx < N || ldb < N) fail(FLAM_ERR_ARG, "FLAM:rskelf_ir_sv:invalidArg: bad dimensions");
+  if (!(tol >= 0) || maxit < 0) fail(FLAM_ERR_ARG, "FLAM:rskelf_ir_sv:invalidArg: need ir_tol >= 0, max_iter >= 0");
+  if (F->Sn_tot > 0) fail(FLAM_ERR_ARG, "FLAM:rskelf_ir_sv:partial: needs a complete factorization");
+  if (F->symm == 'h') fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h'");
+  if (iters) *iters = 0;
+  if (nrhs == 0) return FLAM_OK;
+  if (!B || !X) fail(FLAM_ERR_ARG, "FLAM:rskelf_ir_sv:invalidArg: B and X must not be NULL");
+  const cudaStream_t s = F->s;
+  Workspace& ws = workspace(F->dev, s);
+  F->resolve_pending();
+  int64_t lb = 0;
+  const double* Bd = device_block(B, ldb, N, nrhs, ws.irB, &lb, s);
+  const bool xdev = is_device_ptr(X);
+  double* Xd = X;
+  int64_t lx = ldx;
+  if (!xdev) {
+    ws.irX.ensure(N * nrhs, s);
+    Xd = ws.irX.p;
+    lx = N;
+  }
+  ws.irR.ensure(N * nrhs, s);
+  ws.W.ensure(N * nrhs, s);
+  ws.colsq.ensure(2 * nrhs, s);
+  double* R = ws.irR.p;
+  // X = F \ B
+  CK(cudaMemcpy2DAsync(Xd, sizeof(double) * lx, Bd, sizeof(double) * lb, sizeof(double) * N, nrhs,
+                       cudaMemcpyDeviceToDevice, s));
+  sweeps_on_device(F, Xd, lx, nrhs, ws.W.p, 0, true, kBoth, s);
+  launch_colsq(Bd, N, lb, (int)nrhs, ws.colsq.p + nrhs, s);
+  std::vector<double> bn;
+  double worst = 0;
+  int it = 0;
+  for (;;) {
+    matvec_device(F, Xd, lx, nrhs, Bd, lb, R, N, s);   // R = B - A X
+    launch_colsq(R, N, N, (int)nrhs, ws.colsq.p, s);
+    CK(cudaGetLastError());
+    auto cs = download(ws.colsq.p, 2 * nrhs, s);
+    worst = 0;
+    for (int64_t c = 0; c < nrhs; ++c) {
+      const double rr = cs[nrhs + c] > 0 ? std::sqrt(cs[c] / cs[nrhs + c]) : std::sqrt(cs[c]);
+      if (relres) relres[c] = rr;
+      worst = std::max(worst, rr);
+    }
+    if (!(worst > tol) || it >= maxit) break;
+    sweeps_on_device(F, R, N, nrhs, ws.W.p, 0, true, kBoth, s);   // R = F \ R
+    launch_add_cols(Xd, lx, R, N, N, (int)nrhs, s);                 // X += R
+    F->prof.launches += 1;
+    ++it;
+  }
+  if (iters) *iters = it;
+  if (!xdev) {
+    CK(cudaMemcpy2DAsync(X, sizeof(double) * ldx, Xd, sizeof(double) * lx, sizeof(double) * N, nrhs,
+                         cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  if (!std::isfinite(worst) || worst > tol) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "FLAM:rskelf_ir_sv:notConverged: relative residual %.3e after %d refinement steps",
+             worst, it);
+    g_err = buf;
+    return FLAM_WARN_IR_NOT_CONVERGED;
+  }
+  return FLAM_OK;
+}
+
 template <class Fn>
 flam_status guard(Fn&& fn) {
   try {
@@ -1800,6 +1959,20 @@ flam_status guard(Fn&& fn) {
 }  // namespace
 
 void set_last_error(const char* msg) { g_err = msg; }
+
+cudaError_t ensure_smem_attr(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;   // (kernel, device) -> bytes set
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find({func, dev});
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done[{func, dev}] = bytes;
+  return e;
+}
 
 }  // namespace flam
 
@@ -1952,6 +2125,16 @@ flam_status flam_rskelf_batched(int ninst, const double* x, int d, const int64_t
                                 double occ, double rank_or_tol, const flam_proxy* pxy, const flam_opts* opts,
                                 flam_factor** F) {
   return guard([&] { return create(ninst, x, d, N, A, occ, rank_or_tol, pxy, opts, F); });
+}
+
+flam_status flam_matvec(const flam_factor* F, const double* X, int64_t ldx, int64_t nrhs, const double* B, int64_t ldb,
+                        double* Y, int64_t ldy) {
+  return guard([&] { return matvec(F, X, ldx, nrhs, B, ldb, Y, ldy); });
+}
+
+flam_status flam_rskelf_ir_sv(const flam_factor* F, const double* B, int64_t ldb, double* X, int64_t ldx, int64_t nrhs,
+                              double ir_tol, int max_iter, int* iters, double* relres) {
+  return guard([&] { return ir_solve(F, B, ldb, X, ldx, nrhs, ir_tol, max_iter, iters, relres); });
 }
 
 flam_status flam_rskelf_sv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {

@@ -120,6 +120,13 @@ struct FacDesc {
 // Record the message flam_last_error() returns on this thread (defined with the C ABI).
 void set_last_error(const char* msg);
 
+// Raise `func`'s dynamic shared-memory limit to `bytes` on the current device.
+// Function attributes are per device, so this runs once per (kernel, device),
+// under a lock; a failure is not remembered (the next launch tries again) and
+// leaves the CUDA error pending for the caller's cudaGetLastError().
+// Returns the result of cudaFuncSetAttribute (cudaSuccess once done).
+cudaError_t ensure_smem_attr(const void* func, int bytes);
+
 // Factorization status word bits (device -> host).
 enum StatusBits { ST_NOT_SPD = 1, ST_SINGULAR = 2, ST_RRQR_CAP = 4 };
 

@@ -431,11 +431,7 @@ int64_t compress_scratch_doubles(int n) {
 
 void launch_compress(const CompressArgs& a, int ntask, size_t smem, cudaStream_t s) {
   if (ntask <= 0) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  if (ensure_smem_attr(reinterpret_cast<const void*>(k_compress), 200 * 1024) != cudaSuccess) return;
   k_compress<<<ntask, kThreads, smem, s>>>(a);
 }
 

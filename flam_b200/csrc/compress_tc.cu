@@ -547,11 +547,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
 
 template <int B, int G>
 void launch_b(const CompressArgs& a, int ntask, int nt, size_t smem, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_compress_tc<B, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  if (ensure_smem_attr(reinterpret_cast<const void*>(k_compress_tc<B, G>), 200 * 1024) != cudaSuccess) return;
   k_compress_tc<B, G><<<ntask, nt, smem, s>>>(a);
 }
 

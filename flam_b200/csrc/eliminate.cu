@@ -560,12 +560,9 @@ size_t elim_smem_bytes(int n) {
 int64_t elim_scratch_doubles(int n) { return (int64_t)n * n + (3 * (int64_t)n) / 2 + 2; }
 
 void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_eliminate, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_eliminate_big, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  if (ensure_smem_attr(reinterpret_cast<const void*>(k_eliminate), 200 * 1024) != cudaSuccess ||
+      ensure_smem_attr(reinterpret_cast<const void*>(k_eliminate_big), 200 * 1024) != cudaSuccess)
+    return;
   if (nsmall > 0) k_eliminate<<<nsmall, kThreads, smem, s>>>(a);
   if (nbig > 0) {
     ElimArgs b = a;

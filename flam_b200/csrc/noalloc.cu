@@ -75,13 +75,16 @@ __global__ void k_noalloc_finish(const unsigned char* base, int n, int64_t* k_ou
     for (int e = threadIdx.x; e < k * r; e += blockDim.x) T_out[e] = T[e];
 }
 
-bool on_device(const void* p) {
+// Device (or managed) memory that kernels launched on device `dev` may read: a
+// buffer owned by another GPU is rejected rather than read through a peer mapping.
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes at{};
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+  if (at.type == cudaMemoryTypeManaged) return true;
+  return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
 
 flam_status fail_na(flam_status c, const char* msg) {
@@ -100,17 +103,29 @@ extern "C" flam_status flam_id_noalloc(const double* A, int64_t m, int64_t n, in
   if (!(rank_or_tol >= 0))
     return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidRankOrTol: Rank or tolerance must be nonnegative.");
   if (!(Tmax >= 1)) return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidTmax: Interpolation matrix entry bound must be >= 1.");
-  if (n < 1 || n > kNoAllocN)
-    return fail_na(FLAM_ERR_ARG, "FLAM:id:tooLarge: flam_id_noalloc takes 1 <= n <= FLAM_ID_NOALLOC_NMAX (128) "
+  if (n < 0 || n > kNoAllocN)
+    return fail_na(FLAM_ERR_ARG, "FLAM:id:tooLarge: flam_id_noalloc takes 0 <= n <= FLAM_ID_NOALLOC_NMAX (128) "
                                  "columns; use flam_id for larger matrices");
   if (m < 0 || m > ((int64_t)1 << 30) || (m > 0 && lda < m))
     return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidArg: need 0 <= m <= 2^30 and lda >= m");
-  if (!k || !perm || !T || (m > 0 && !A)) return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidArg: NULL pointer");
-  if ((m > 0 && !on_device(A)) || !on_device(k) || !on_device(perm) || !on_device(T) || (niter && !on_device(niter)))
-    return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidArg: flam_id_noalloc needs device pointers for A and every output");
+  if (!k || (n > 0 && (!perm || !T || (m > 0 && !A))))
+    return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidArg: NULL pointer");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return fail_na(FLAM_ERR_CUDA, "FLAM:gpu:cuda: cudaGetDevice failed");
+  if (!on_device(k, dev) || (niter && !on_device(niter, dev)) ||
+      (n > 0 && (!on_device(perm, dev) || !on_device(T, dev) || (m > 0 && !on_device(A, dev)))))
+    return fail_na(FLAM_ERR_ARG, "FLAM:id:invalidArg: flam_id_noalloc needs device pointers on the current device "
+                                 "for A and every output");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {   // no columns: k = 0, nothing to permute (as flam_id)
+    if (cudaMemsetAsync(k, 0, sizeof(int64_t), s) != cudaSuccess ||
+        (niter && cudaMemsetAsync(niter, 0, sizeof(int64_t), s) != cudaSuccess)) {
+      cudaGetLastError();
+      return fail_na(FLAM_ERR_CUDA, "FLAM:gpu:cuda: cudaMemsetAsync failed in flam_id_noalloc");
+    }
+    return FLAM_OK;
+  }
   unsigned char* base = nullptr;
   {
     // First call on this device (with it current): look up the array's device
@@ -128,7 +143,6 @@ extern "C" flam_status flam_id_noalloc(const double* A, int64_t m, int64_t n, in
     }
     base = g_addr[dev];
   }
-  cudaStream_t s = (cudaStream_t)stream;
   CompressTask t{};
   t.slf_off = 0;
   t.cand_off = 0;

@@ -284,7 +284,9 @@ FLAM_HD inline int rrqr_serial(double* R, int64_t rs, int64_t cs, int n, int k, 
     if (k == 0) break;
   }
   *niter_out = niter;
-  *capped = (!conv && k > 0 && niter >= kRrqrCapH) ? 1 : 0;
+  // id.m:232-235 warns whenever the loop ends unconverged, i.e. at rrqr_iter swaps
+  // (or at the device's hard cap when rrqr_iter is Inf)
+  *capped = (!conv && k > 0 && (niter >= kRrqrCapH || (rrqr_iter >= 0 && niter >= rrqr_iter))) ? 1 : 0;
   return k;
 }
 

@@ -351,11 +351,7 @@ void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t
   // products (the solves work in place), kTs columns each
   const int64_t slot = (int64_t)(kmax + (a.op >= 2 ? 2 : 1) * rmax) * kTs;
   const size_t need = sizeof(double) * (size_t)slot;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  if (ensure_smem_attr(reinterpret_cast<const void*>(k_sweep), 200 * 1024) != cudaSuccess) return;
   const int64_t nblk = (int64_t)nfac * ((a.nrhs + kTs - 1) / kTs);
   const unsigned g = (unsigned)nblk;
   if (need <= 200 * 1024) {

@@ -52,7 +52,8 @@ typedef enum {
   FLAM_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
   FLAM_ERR_ID_CHECK = 7,     /* posterior ID residual check failed */
   FLAM_WARN_RRQR_MAXITER = 100, /* FLAM:id:maxIterCount (factor is still valid) */
-  FLAM_WARN_SINGULAR = 101      /* an LU pivot of a redundant block was exactly zero */
+  FLAM_WARN_SINGULAR = 101,     /* an LU pivot of a redundant block was exactly zero */
+  FLAM_WARN_IR_NOT_CONVERGED = 102 /* refinement stopped above ir_tol (X is the last iterate) */
 } flam_status;
 
 /* Kernel registry: the matrix entry is A(i,j) = scale * w_j * K(x_i, x_j) for
@@ -130,21 +131,28 @@ FLAM_API flam_status flam_id(const double* A, int64_t m, int64_t n, int64_t lda,
 /* Column limit of flam_id_noalloc. */
 #define FLAM_ID_NOALLOC_NMAX 128
 
+/* The device's RRQR loop stops after this many swaps when rrqr_iter is Inf. */
+#define FLAM_RRQR_HARD_CAP 4096
+
 /* flam_id without device allocation -- no counterpart in the reference.
  * For callers that cannot allocate device memory (a MEX/oct gateway running
  * inside a MATLAB or Octave session whose GPU memory manager owns the device
  * heap, a thread that must not enter cudaMalloc/cudaFree): the caller passes
- * DEVICE pointers for the m x n matrix A (leading dimension lda) and for every
- * output -- *k, perm (n entries, sk = perm[0:k], rd = perm[k:n]), T (room for
- * n*n/4 + 1 doubles; written k x (n-k), leading dimension k) and *niter (may be
- * NULL) -- and the work runs asynchronously on `stream` (NULL: legacy default
- * stream).  Scratch is a 64 KiB array compiled into the library, resident on
- * every GPU that loads it until the process exits; n is limited to
+ * DEVICE pointers on the current device for the m x n matrix A (leading
+ * dimension lda) and for every output -- *k, perm (n entries, sk = perm[0:k],
+ * rd = perm[k:n]), T (room for n*n/4 + 1 doubles; written k x (n-k), leading
+ * dimension k) and *niter (may be NULL) -- and the work runs asynchronously on
+ * `stream` (NULL: legacy default stream).  Because the call does not wait for
+ * the GPU it cannot return flam_id's FLAM_WARN_RRQR_MAXITER: the RRQR loop
+ * stopped unconverged at its limit exactly when *niter equals rrqr_iter (or
+ * FLAM_RRQR_HARD_CAP when rrqr_iter < 0).  n = 0 writes *k = *niter = 0.
+ * Scratch is a 64 KiB array compiled into the library, resident on every GPU
+ * that loads it until the process exits; n is limited to
  * FLAM_ID_NOALLOC_NMAX (larger n returns FLAM_ERR_ARG).  The first call on a
  * device looks up that array's address with the device current; make that
  * first call before any stream capture.  All calls share the array: calls that
  * overlap on one GPU race and must be serialised by the caller.
- * Same algorithm and results as flam_id (core/id.m:44-248). */
+ * Same algorithm and results as flam_id. */
 FLAM_API flam_status flam_id_noalloc(const double* A, int64_t m, int64_t n, int64_t lda, double rank_or_tol,
                                      double Tmax, int64_t rrqr_iter, int64_t* k, int64_t* perm, double* T,
                                      int64_t* niter, void* stream);
@@ -230,6 +238,26 @@ FLAM_API flam_status flam_rskelf_partial_sv(const flam_factor* F, double* X, int
 /* Y = rskelf_partial_mv(F, X, mvfun, trans), in place.  rskelf/rskelf_partial_mv.m:23-62. */
 FLAM_API flam_status flam_rskelf_partial_mv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans,
                                             flam_skel_fn fn, void* ctx);
+
+/* Y = A X, or Y = B - A X when B is not NULL: the handle's registry matrix (block
+ * diagonal over the instances of a batched handle) applied in FP64, evaluated on the
+ * fly -- the O(N^2) product the reference's tests form from A(I,J) to measure errors
+ * (rskelf/test/ie_circle.m:47-48, ie_ellipse.m:51-80).  X, B, Y are N x nrhs with
+ * leading dimensions ldx, ldb, ldy, host or device memory; Y may not alias X.
+ * Errors: FLAM:gpu:noMatrix for imported factors (no matrix). */
+FLAM_API flam_status flam_matvec(const flam_factor* F, const double* X, int64_t ldx, int64_t nrhs, const double* B,
+                                 int64_t ldb, double* Y, int64_t ldy);
+
+/* X = A \ B by iterative refinement on the factorization F of A: X = F \ B
+ * (rskelf_sv), then X += F \ (B - A X) with the FP64 residual of flam_matvec
+ * until max_j ||B_j - A X_j|| / ||B_j|| <= ir_tol or max_iter refinement steps.
+ * F may be a loose (larger rank_or_tol) factorization; the returned error is the
+ * FP64 relative residual per column (relres, nrhs entries, may be NULL), and
+ * *iters the refinement steps taken.  FLAM_WARN_IR_NOT_CONVERGED when the
+ * tolerance was not met.  No counterpart in the reference (its users pass
+ * rskelf_sv as a preconditioner to an iterative solver, ie_square1.m:102). */
+FLAM_API flam_status flam_rskelf_ir_sv(const flam_factor* F, const double* B, int64_t ldb, double* X, int64_t ldx,
+                                       int64_t nrhs, double ir_tol, int max_iter, int* iters, double* relres);
 
 /* Sizes of a handle. */
 typedef struct {

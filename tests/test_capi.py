@@ -28,9 +28,11 @@ def test_library_exports_every_declared_symbol():
     assert b"sm_100a" in L.flam_version()
 
 
-def test_library_is_built_for_sm100a():
-    so = open(_lib.LIB_PATH, "rb").read()
-    assert b"sm_100a" in so
+def test_build_recipe_targets_sm100a_only():
+    """Every translation unit and the link use one -gencode: sm_100a code, no PTX for other arches."""
+    from flam_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert set(build.SOURCES) == {f for f in os.listdir(build.CSRC) if f.endswith(".cu")}
 
 
 def test_bad_arguments_fail_before_the_device():
