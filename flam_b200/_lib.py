@@ -44,7 +44,8 @@ class FlamProxy(C.Structure):
 class FlamOpts(C.Structure):
     _fields_ = [("lvlmax", C.c_int), ("ext", C.c_void_p), ("Tmax", C.c_double), ("rrqr_iter", C.c_int64),
                 ("symm", C.c_char), ("stop", C.c_int), ("verb", C.c_int), ("stream", C.c_void_p),
-                ("profile", C.c_int)]
+                ("profile", C.c_int), ("sketch", C.c_int), ("sketch_p", C.c_int), ("sketch_guard", C.c_int),
+                ("sketch_seed", C.c_uint), ("predictor", C.c_void_p)]
 
 
 class FlamInfo(C.Structure):
@@ -57,7 +58,7 @@ class FlamProf(C.Structure):
     _fields_ = [("launches", C.c_int64), ("n_compress", C.c_int64), ("n_elim", C.c_int64), ("n_sweep", C.c_int64),
                 ("t_compress", C.c_double), ("t_elim", C.c_double), ("t_sweep", C.c_double),
                 ("flop_compress", C.c_double), ("flop_elim", C.c_double), ("flop_sweep", C.c_double),
-                ("byte_sweep", C.c_double)]
+                ("byte_sweep", C.c_double), ("n_sketch", C.c_int64), ("n_sketch_redo", C.c_int64)]
 
 
 class FlamError(RuntimeError):

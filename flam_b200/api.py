@@ -26,7 +26,8 @@ import numpy as np
 from . import _lib
 from .registry import Kernel, Proxy
 
-_OPT_KEYS = {"lvlmax", "ext", "Tmax", "rrqr_iter", "symm", "stop", "verb", "stream", "profile"}
+_OPT_KEYS = {"lvlmax", "ext", "Tmax", "rrqr_iter", "symm", "stop", "verb", "stream", "profile", "sketch", "sketch_p",
+             "sketch_guard", "sketch_seed", "predictor"}
 
 
 def _c_opts(opts):
@@ -57,6 +58,12 @@ def _c_opts(opts):
             o.stream = v
         elif k == "profile":
             o.profile = int(bool(v))
+        elif k in ("sketch", "sketch_p", "sketch_guard"):
+            setattr(o, k, int(v))
+        elif k == "sketch_seed":
+            o.sketch_seed = int(v) & 0xFFFFFFFF
+        elif k == "predictor":
+            o.predictor = None if v is None else (v.handle if hasattr(v, "handle") else v)
     return o, keep
 
 

@@ -28,6 +28,7 @@
 #include "kernels.cuh"
 #include "matvec.cuh"
 #include "scan.cuh"
+#include "sketch.cuh"
 #include "tree.cuh"
 
 namespace flam {
@@ -176,6 +177,11 @@ struct Workspace {
   DBuf<CompressOut> cout;
   // FP64 products with the registry matrix and iterative refinement (matvec.cu)
   DBuf<MatvecTile> mvt;
+  // sketched compression: row sketches, their tasks, rows of K per box, boxes redone exactly
+  DBuf<double> ypool;
+  DBuf<SketchTask> sktask;
+  DBuf<CompressTask> skfilt, redo_task;
+  DBuf<int32_t> mrows, redo_idx;
   DBuf<double> irB, irX, irR, irW, colsq;
   cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
   // side streams for the independent launches of one step (the kernel shapes of a
@@ -257,6 +263,12 @@ struct Workspace {
     permpool_b.release(s);
     for (auto* b : {&tpool, &scratch, &mpool[0], &mpool[1], &W, &tmp, &irB, &irX, &irR, &irW, &colsq}) b->release(s);
     mvt.release(s);
+    ypool.release(s);
+    sktask.release(s);
+    skfilt.release(s);
+    redo_task.release(s);
+    mrows.release(s);
+    redo_idx.release(s);
     cpool.release(s);
     permpool.release(s);
     status.release(s);
@@ -965,6 +977,30 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       const char* e = std::getenv("FLAM_SPLIT_MIN_N");
       return e ? std::max(1, std::atoi(e)) : 32;
     }();
+    // sketched compression (opts.sketch): boxes of at most kSketchMaxN points whose block
+    // has more rows than the sketch take Y = Omega K (w rows) and an ID of Y
+    std::vector<int> pred_k;   // per box: the rank predictor's estimate (empty: no predictor)
+    std::vector<int> skw(nb, 0);
+    std::vector<int64_t> yoff(nb, -1);
+    int64_t ytop = 0;
+    if (o.sketch) {
+      const int sp = o.sketch_p;
+      for (int q = 0; q < nb; ++q) {
+        const int n = (int)nslf[q];
+        if (n == 0 || n > kSketchMaxN) continue;
+        const int32_t b = boxes[q];
+        const int i = F.binst[b];
+        const bool use_proxy = F.depth[b] > 2 && F.iph[i].pkind != P_NONE;
+        const int64_t mcap = (F.symm == 'n' ? 2 : 1) * ncand[q] +
+                             (use_proxy ? (F.iph[i].two_sided ? 2 : 1) * (int64_t)F.npxy : 0);
+        const int kest = pred_k.empty() ? n : std::min(n, pred_k[q]);
+        const int w = std::min(std::max(kest + sp, 8), kSketchMaxW);
+        if (mcap <= w) continue;   // the block is no taller than its sketch: exact ID
+        skw[q] = w;
+        yoff[q] = ytop;
+        ytop += (int64_t)w * n;
+      }
+    }
     int nparts = 1;
     while (nparts * 2 <= split_max && nparts * 2 * nb <= split_ctas) nparts *= 2;
     std::vector<char> split(nb, 0);
@@ -999,7 +1035,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       const int64_t mcap = (F.symm == 'n' ? 2 : 1) * ncand[q] +
                            (use_proxy ? (F.iph[i].two_sided ? 2 : 1) * (int64_t)F.npxy : 0);
       // as many parts (up to nparts) as leave each part at least one row panel
-      if (nparts > 1 && tc && n > split_min_n) {
+      if (nparts > 1 && tc && n > split_min_n && skw[q] == 0) {
         const int64_t ph = (int64_t)compress_tc_rows(n) * compress_tc_group(n);
         int np = nparts;
         while (np > 1 && mcap < np * ph) np /= 2;
@@ -1040,7 +1076,43 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // task segments: [whole boxes | filter of split boxes | parts | merge level 0 | level 1 ...]
     std::vector<CompressTask> cts;
     cts.reserve(nb * 3);
-    for (int q : ord) cts.push_back(ct[q]);
+    // sketched boxes: their filter and sketch tasks, and the ID of Y in place of K's rows
+    std::vector<SketchTask> skt;
+    std::vector<CompressTask> skf;
+    std::vector<int> sk_of(nb, -1);
+    const int sk_guard = std::max(0, o.sketch_guard);
+    for (int q : ord) {
+      if (skw[q] == 0) {
+        cts.push_back(ct[q]);
+        continue;
+      }
+      const CompressTask& c0 = ct[q];
+      SketchTask u{};
+      u.slf_off = c0.slf_off;
+      u.cand_off = c0.cand_off;
+      u.y_off = yoff[q];
+      u.perm_off = c0.perm_off;
+      u.n = c0.n;
+      u.w = skw[q];
+      u.inst = c0.inst;
+      u.out_idx = c0.out_idx;
+      u.box = c0.box;
+      u.flags = c0.flags & 1;
+      for (int c = 0; c < kMaxDim; ++c) {
+        u.ctr[c] = c0.ctr[c];
+        u.l[c] = c0.l[c];
+      }
+      sk_of[q] = (int)skt.size();
+      skt.push_back(u);
+      skf.push_back(c0);
+      CompressTask v = c0;
+      v.flags = 0;
+      v.ncand = skw[q];
+      v.ax_off = yoff[q];
+      v.ax_rows = skw[q];
+      v.ax_guard = sk_guard;
+      cts.push_back(v);
+    }
     std::vector<int> seg{(int)cts.size()};
     std::vector<int> sord;
     for (int q = 0; q < nb; ++q)
@@ -1091,6 +1163,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ca.Aexp = nullptr;
     ca.lda = 0;
     ca.mfilt = ws.mfilt.p;
+    if (ytop > 0) ws.ypool.ensure(ytop, s);
+    ca.ypool = ws.ypool.p;
     F.prof.launches += 2 + 1;  // two id gathers, compress
     F.prof.n_compress += 1;
     if (prof) {
@@ -1139,6 +1213,30 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       }
       if (nuse > 1) ws.join_to(s, nuse);
     };
+    if (!skt.empty()) {   // neighbour filter and row sketch of the sketched boxes, before their IDs
+      ws.mrows.ensure(nb, s);
+      ws.sktask.upload(skt, s);
+      ws.skfilt.upload(skf, s);
+      CompressArgs cf = ca;
+      cf.tasks = ws.skfilt.p;
+      launch_filter(cf, (int)skf.size(), s);
+      SketchArgs sa{};
+      sa.P = P;
+      sa.tasks = ws.sktask.p;
+      sa.ipool = F.ipool.p;
+      sa.cpool = cpool.p;
+      sa.mfilt = ws.mfilt.p;
+      sa.ypool = ws.ypool.p;
+      sa.mrows = ws.mrows.p;
+      sa.symm_n = F.symm == 'n' ? 1 : 0;
+      sa.seed = o.sketch_seed;
+      sa.status = status.p;
+      size_t smx = 0;
+      for (const SketchTask& u : skt) smx = std::max(smx, sketch_smem_bytes(u.n, u.w));
+      launch_sketch(sa, (int)skt.size(), smx, s);
+      F.prof.launches += 2;
+      F.prof.n_sketch += (int64_t)skt.size();
+    }
     launch_segment(0, seg[0]);
     if (seg.size() > 1) {
       CompressArgs cf = ca;
@@ -1151,6 +1249,55 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     CK(cudaGetLastError());
     if (prof) CK(cudaEventRecord(pe[1], s));
     auto co = download(cout.p, nb, s);
+    if (!skt.empty()) {
+      // posterior check of the sketched IDs: a box whose rank came within sketch_guard of
+      // its sketch rows is redone with the exact ID of K (from the pull-up order, with the
+      // candidates the filter kept)
+      std::vector<int> redo;
+      for (int q = 0; q < nb; ++q)
+        if (skw[q] > 0 && (co[q].status & ST_ID_CHECK)) redo.push_back(q);
+      auto mr = download(ws.mrows.p, nb, s);
+      for (int q = 0; q < nb; ++q)
+        if (skw[q] > 0) co[q].m = mr[q];   // rows of K, for the work accounting
+      if (!redo.empty()) {
+        auto mf = download(ws.mfilt.p, nb, s);
+        std::vector<int32_t> ridx;
+        std::vector<CompressTask> rt;
+        int nmx = 0;
+        for (int q : redo) {
+          ridx.push_back(sk_of[q]);
+          CompressTask v = ct[q];
+          v.flags &= ~2;          // candidates already filtered
+          v.ncand = mf[q];
+          rt.push_back(v);
+          nmx = std::max(nmx, (int)nslf[q]);
+        }
+        std::stable_sort(rt.begin(), rt.end(),
+                         [&](const CompressTask& x, const CompressTask& y) { return kkey_n(x.n) < kkey_n(y.n); });
+        ws.redo_idx.upload(ridx, s);
+        ws.redo_task.upload(rt, s);
+        launch_unpermute(ws.redo_idx.p, (int)ridx.size(), ws.sktask.p, F.ipool.p, permpool.p, nmx, s);
+        for (size_t b0 = 0; b0 < rt.size();) {
+          const int key = kkey_n(rt[b0].n);
+          size_t b1 = b0;
+          size_t sm = 16;
+          while (b1 < rt.size() && kkey_n(rt[b1].n) == key) {
+            if (rt[b1].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(rt[b1].n));
+            ++b1;
+          }
+          CompressArgs cr = ca;
+          cr.tasks = ws.redo_task.p + b0;
+          launch_compress_tc(cr, (int)(b1 - b0), key / 1000, (key / 10) % 100, key % 10, sm, s);
+          F.prof.launches += 1;
+          b0 = b1;
+        }
+        CK(cudaGetLastError());
+        F.prof.launches += 1;
+        F.prof.n_sketch_redo += (int64_t)redo.size();
+        auto co2 = download(cout.p, nb, s);
+        for (int q : redo) co[q] = co2[q];
+      }
+    }
 
     // ---- elimination plan
     std::vector<ElimTask> et(nb);
@@ -1989,6 +2136,11 @@ void flam_opts_default(flam_opts* o) {
   o->verb = 0;
   o->stream = nullptr;
   o->profile = 0;
+  o->sketch = 0;
+  o->sketch_p = 8;
+  o->sketch_guard = 2;
+  o->sketch_seed = 0x5eed1234u;
+  o->predictor = nullptr;
 }
 
 flam_status flam_rskelf(const double* x, int d, int64_t N, const flam_kernel* A, double occ, double rank_or_tol,

@@ -76,6 +76,13 @@ struct CompressTask {
   int32_t part, nparts;
   int32_t pad_;
   int64_t rsrc_off;
+  // Sketched form: with ax_rows > 0 the rows of the block are the explicit ax_rows x n
+  // matrix (column-major, leading dimension ax_rows) at ax_off of the sketch pool -- the
+  // box's row sketch Y = Omega K -- instead of rows generated from the points, and the
+  // result is flagged ST_ID_CHECK when the rank exceeds ax_rows - ax_guard.
+  int64_t ax_off;
+  int32_t ax_rows;
+  int32_t ax_guard;
 };
 
 // Per-box results of the compress kernel.
@@ -128,7 +135,9 @@ void set_last_error(const char* msg);
 cudaError_t ensure_smem_attr(const void* func, int bytes);
 
 // Factorization status word bits (device -> host).
-enum StatusBits { ST_NOT_SPD = 1, ST_SINGULAR = 2, ST_RRQR_CAP = 4 };
+// ST_ID_CHECK: a sketched ID used (nearly) all of its sketch rows, so the sketch may
+// have cut the numerical rank; ST_TIMEOUT: a bounded device wait gave up.
+enum StatusBits { ST_NOT_SPD = 1, ST_SINGULAR = 2, ST_RRQR_CAP = 4, ST_ID_CHECK = 8, ST_TIMEOUT = 16 };
 
 // ---------------------------------------------------------------- device helpers
 #ifdef __CUDACC__

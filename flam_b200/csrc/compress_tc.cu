@@ -193,7 +193,10 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   const int m1 = mode != 0 ? a.mfilt[t.out_idx] : ((t.flags & 2) ? filter_candidates(t, P, ip, cand, s_cnt) : t.ncand);
   const int nrep = a.symm_n ? 2 : 1;
   const int npr = (t.flags & 1) ? (ip.two_sided ? 2 * P.npxy : P.npxy) : 0;
-  const int m = a.Aexp ? t.ncand : nrep * m1 + npr;
+  // explicit rows: flam_id's matrix, or this box's row sketch
+  const double* Ax = a.Aexp ? a.Aexp : (t.ax_rows > 0 ? a.ypool + t.ax_off : nullptr);
+  const int64_t lda = a.Aexp ? a.lda : t.ax_rows;
+  const int m = a.Aexp ? t.ncand : (Ax ? t.ax_rows : nrep * m1 + npr);
   const int mn = min(m, n);
 
   // ---- (2) TSQR: fold PH-row panels of K into R0; G threads per column.  A part of
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   __syncthreads();
   double p[B];
   for (int p0 = rbeg; p0 < rend; p0 += PH) {
-    if (!a.Aexp && !Rsrc && tid < PH) {
+    if (!Ax && !Rsrc && tid < PH) {
       const int rho = p0 + tid < rend ? p0 + tid : m;   // rows past the part are zero
       int ty = 3;
       int64_t q = -1;
@@ -249,9 +252,9 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
       if (Rsrc) {
 #pragma unroll
         for (int i = 0; i < B; ++i) p[i] = (r0 + i < rend) ? Rsrc[(int64_t)(r0 + i) * ld + col] : 0.0;
-      } else if (a.Aexp) {
+      } else if (Ax) {
 #pragma unroll
-        for (int i = 0; i < B; ++i) p[i] = (r0 + i < m) ? a.Aexp[(r0 + i) + (int64_t)col * a.lda] : 0.0;
+        for (int i = 0; i < B; ++i) p[i] = (r0 + i < m) ? Ax[(r0 + i) + (int64_t)col * lda] : 0.0;
       } else {
 #pragma unroll
         for (int i = 0; i < B; ++i) {
@@ -542,7 +545,12 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     double* T = a.tpool + t.T_off;
     for (int i = 0; i < k; ++i) T[i + (int64_t)(c - k) * k] = R[(int64_t)i * ld + c];
   }
-  if (tid == 0) *out = CompressOut{k, m, s_niter, s_cap ? (int)ST_RRQR_CAP : 0};
+  if (tid == 0) {
+    int st = s_cap ? (int)ST_RRQR_CAP : 0;
+    // sketched ID check: a rank within ax_guard of the sketch's rows may have been cut by the sketch
+    if (t.ax_rows > 0 && k > t.ax_rows - t.ax_guard) st |= ST_ID_CHECK;
+    *out = CompressOut{k, m, s_niter, st};
+  }
 }
 
 template <int B, int G>

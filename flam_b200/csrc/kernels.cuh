@@ -21,6 +21,7 @@ struct CompressArgs {
   const double* Aexp;  // explicit m x n matrix (flam_id); rows are generated from points when null
   int64_t lda;
   int32_t* mfilt;      // per box (out_idx): candidates kept by the neighbour filter (row-split form)
+  const double* ypool; // row sketches of the sketched boxes (CompressTask::ax_off)
 };
 
 size_t compress_smem_bytes(int n);

@@ -40,6 +40,9 @@ constexpr size_t kOffPerm = kOffIds + 8 * kNoAllocN;                 // n int32 
 constexpr size_t kOffT = (kOffPerm + 4 * kNoAllocN + 255) / 256 * 256;  // n*n/4+1 doubles
 constexpr size_t kEnd = kOffT + 8 * ((size_t)kNoAllocN * kNoAllocN / 4 + 1);
 static_assert(kEnd <= kNoAllocBytes, "no-alloc scratch layout exceeds the array");
+static_assert(sizeof(CompressTask) <= kOffOut - kOffTask && sizeof(CompressOut) <= kOffInst - kOffOut &&
+                  sizeof(InstParams) <= kOffDummy - kOffInst,
+              "no-alloc scratch sections too small for their records");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 

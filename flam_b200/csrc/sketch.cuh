@@ -1,0 +1,44 @@
+// Randomized row sketch of the compression blocks on the tensor cores (sketch.cu).
+#pragma once
+#include "common.cuh"
+
+namespace flam {
+
+// Boxes up to this many points are sketched (two 128-column tiles of tensor memory);
+// larger boxes take the exact compression.
+constexpr int kSketchMaxN = 256;
+constexpr int kSketchMaxW = 256;
+
+// One box of a factorization step in the sketched form.
+struct SketchTask {
+  int64_t slf_off;   // ids in ipool (pull-up order)
+  int64_t cand_off;  // neighbour candidates in cpool, already filtered (count in mfilt[out_idx])
+  int64_t y_off;     // Y = Omega K (w x n, column-major, leading dimension w) in the sketch pool
+  int64_t perm_off;  // the compression's local permutation of this box (permpool)
+  int32_t n, w;
+  int32_t inst, out_idx;
+  int32_t box, flags;  // flags bit0: proxy rows (level > 2)
+  double ctr[kMaxDim];
+  double l[kMaxDim];
+};
+
+struct SketchArgs {
+  Problem P;
+  const SketchTask* tasks;
+  const int64_t* ipool;
+  const int64_t* cpool;
+  const int32_t* mfilt;   // filtered candidate count per out_idx
+  double* ypool;
+  int32_t* mrows;         // per out_idx: rows of K the sketch compressed
+  int symm_n;
+  uint32_t seed;
+  int32_t* status;        // OR of StatusBits (ST_TIMEOUT)
+};
+
+size_t sketch_smem_bytes(int n, int w);
+void launch_sketch(const SketchArgs& a, int ntask, size_t smem, cudaStream_t s);
+// Boxes idx[0, nidx) of tasks: restore the slf order the compression permuted (perm_off).
+void launch_unpermute(const int32_t* idx, int nidx, const SketchTask* tasks, int64_t* ipool, const int32_t* permpool,
+                      int nmax, cudaStream_t s);
+
+}  // namespace flam

@@ -103,6 +103,19 @@ typedef struct {
   int verb;              /* 1: print the per-level table                  (rskelf.m:120) */
   void* stream;          /* cudaStream_t the handle runs on (NULL: default stream) */
   int profile;           /* 1: time every launch with CUDA events (see flam_profile) */
+  /* Sketched (mixed-precision) compression -- not in the reference.  0: the reference's
+   * ID of the full block K (id.m).  1: the ID of a row sketch Y = Omega K (Omega w x m,
+   * +-1 entries) formed in FP32 on the tensor cores (K split into two TF32 parts),
+   * with the FP64 pivoted QR, rank and R11 \ R12 on Y; boxes of more than 256 points use
+   * the exact ID.  A box whose rank comes within sketch_guard of w is redone exactly
+   * (the posterior check).  Meant for loose tolerances (>= ~1e-7: the sketch carries
+   * ~21 bits) followed by flam_rskelf_ir_sv. */
+  int sketch;
+  int sketch_p;          /* sketch rows beyond the rank estimate (default 8; w >= 8) */
+  int sketch_guard;      /* posterior check margin in rows (default 2) */
+  unsigned sketch_seed;  /* seed of Omega */
+  const void* predictor; /* flam_predictor* giving each box's rank estimate, or NULL:
+                            w = n + sketch_p (never below the rank) */
 } flam_opts;
 
 typedef struct flam_factor flam_factor;
@@ -323,6 +336,8 @@ typedef struct {
   double t_compress, t_elim, t_sweep;     /* seconds (0 unless profiling is on) */
   double flop_compress, flop_elim, flop_sweep;
   double byte_sweep;
+  int64_t n_sketch;        /* boxes whose ID came from a row sketch (opts.sketch) */
+  int64_t n_sketch_redo;   /* of those, boxes the posterior check sent to the exact ID */
 } flam_prof;
 
 FLAM_API flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset);

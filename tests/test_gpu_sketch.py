@@ -1,0 +1,72 @@
+"""Sketched (mixed-precision) compression: the ID of a row sketch Y = Omega K formed in
+FP32 on the tensor cores (tcgen05 kind::tf32), FP64 pivoted QR / rank / R11 \\ R12 on Y
+(core/id.m:102-114 applied to Y), the posterior check that redoes a box exactly, and FP64
+iterative refinement back to the FP64 tolerance."""
+import numpy as np
+import pytest
+
+import flam_b200 as fb
+from flam_b200 import problems
+from oracle import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def _ranks(F):
+    fac = F.factors()["factors"]
+    return np.array([len(f["sk"]) for f in fac]), np.array([len(f["rd"]) for f in fac])
+
+
+@pytest.mark.parametrize("case", ["star", "sphere", "matern"])
+def test_sketched_factorization_matches_exact_ranks_and_tolerance(case):
+    if case == "star":
+        (x, A, pxy), (xo, Ao, po), symm = problems.star(6000, seed=5), configs.star(6000, seed=5), "n"
+    elif case == "sphere":
+        (x, A, pxy), (xo, Ao, po), symm = (problems.sphere(5000, p=128, seed=1), configs.sphere(5000, p=128, seed=1),
+                                           "n")
+    else:
+        (x, A, pxy), (xo, Ao, po), symm = (problems.matern_cube(4000, seed=2, p=32, p_rad=4),
+                                           configs.matern_cube(4000, seed=2, p=32, p_rad=4), "p")
+    tol = 1e-6
+    Fe = fb.rskelf(A, x, 64, tol, pxy, dict(symm=symm))
+    Fs = fb.rskelf(A, x, 64, tol, pxy, dict(symm=symm, sketch=1, profile=True))
+    prof = Fs.profile()
+    assert prof["n_sketch"] > 0 and prof["n_sketch_redo"] == 0
+    ke, re_ = _ranks(Fe)
+    ks, rs = _ranks(Fs)
+    # same tree, same boxes per step; ranks of the sketched ID within a few of the exact ID's
+    assert Fe.info()["nstep"] == Fs.info()["nstep"]
+    assert abs(int(ks.sum()) - int(ke.sum())) <= 0.05 * ke.sum() + 5
+    N = x.shape[1]
+    D = Ao.dense()
+    B = np.asfortranarray(np.random.default_rng(1).standard_normal((N, 2)))
+    for F in (Fe, Fs):
+        X = fb.rskelf_sv(F, B)
+        assert np.linalg.norm(D @ X - B) / np.linalg.norm(B) < 1e3 * tol
+    X, it, rel = fb.rskelf_ir_sv(Fs, B, ir_tol=1e-10, max_iter=10)
+    r = np.linalg.norm(D @ X - B, axis=0) / np.linalg.norm(B, axis=0)
+    assert r.max() <= 1e-10 and rel.max() <= 1e-10
+
+
+def test_posterior_check_redoes_boxes_whose_rank_fills_the_sketch():
+    x, A, pxy = problems.star(5000, seed=3)
+    xo, Ao, po = configs.star(5000, seed=3)
+    tol = 1e-6
+    Fe = fb.rskelf(A, x, 64, tol, pxy, dict(symm="n"))
+    # w = n - 40 rows: boxes of rank above w - 2 must go back to the exact ID
+    Fs = fb.rskelf(A, x, 64, tol, pxy, dict(symm="n", sketch=1, sketch_p=-40, sketch_guard=2, profile=True))
+    prof = Fs.profile()
+    assert prof["n_sketch_redo"] > 0
+    ke, _ = _ranks(Fe)
+    ks, _ = _ranks(Fs)
+    assert abs(int(ks.sum()) - int(ke.sum())) <= 0.05 * ke.sum() + 5
+    D = Ao.dense()
+    B = np.asfortranarray(np.random.default_rng(2).standard_normal((5000, 2)))
+    X = fb.rskelf_sv(Fs, B)
+    assert np.linalg.norm(D @ X - B) / np.linalg.norm(B) < 1e3 * tol
+
+
+def test_sketch_off_is_the_exact_path():
+    x, A, pxy = problems.star(3000, seed=4)
+    F0 = fb.rskelf(A, x, 64, 1e-8, pxy, dict(symm="n", profile=True))
+    assert F0.profile()["n_sketch"] == 0
