@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""rskelf factor + solve throughput (DOF/s) on B200.
+"""rskelf factor+solve throughput (DOF/s) on B200: plain FP64 and the chosen form.
 
 Workload (one "step"): build the tree, factor, and solve 256 right-hand sides
 for N = 262144 points on the star curve r(t) = 1 + 0.3 cos 5t with t drawn
@@ -10,11 +10,21 @@ instance (seed = rank), so per-GPU work is fixed as the GPU count grows.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl flam|reference]
 
-``value``: DOF/s with the inputs resident in HBM (CUDA events on the launch
-stream, max over ranks).  ``e2e``: the same through the public API with host
-buffers (pinned), host<->device copies inside the timed region.
-``--impl reference`` times the CPU restatement of the reference algorithm
-(the reference itself is MATLAB and does not run here) on a bounded sample.
+value     plain FP64 DOF/s with the inputs resident in HBM (CUDA events on the
+          launch stream, max over ranks).
+e2e       the same through the public API with pinned host buffers, the
+          host<->device copies inside the timed region.
+accuracy  the FP64 relative residual of all 256 solutions, from the library's
+          on-the-fly FP64 matvec (not timed).
+chosen_form (rank 0)  the metric's comparison: the mixed-precision form -- row
+          sketches formed in FP32/TF32 on the tensor cores, sketch widths from the
+          learned rank predictor, FP64 pivots and R11 \\ R12, the factorization at a
+          loose tolerance refined in FP64 to 1e-10 against the FP64 matvec --
+          against plain FP64 at 1e-10, on this workload and on the 3D sphere of the
+          mixed-precision configuration (Fibonacci points with a random rotation,
+          3D Laplace, 256-point proxy sphere, 64 RHS), each with its FP64 error.
+--impl reference  times the CPU restatement of the reference algorithm (the
+          reference is MATLAB and does not run here) on a bounded sample.
 """
 import argparse
 import json
@@ -34,11 +44,14 @@ METRIC = "rskelf factor+solve DOF/s at 1e-10 rel. err: chosen form vs plain FP64
 UNIT = "DOF/s"
 N_DEF, NRHS_DEF, OCC, TOL = 262144, 256, 64, 1e-10
 CPU_SAMPLE_N = 16384
-# DRAM bytes (read + write) per compress step of the N=262144 workload: one ncu capture
-# of every k_compress_tc launch of an N=65536 factorization (156.4 MB over its level
-# steps; profiles/k_compress_tc_star65536_top.md) scaled by the box count (x4) and
-# divided by this workload's 23 steps.
+# DRAM bytes (read + write) per compress step of the N=262144 workload, from one ncu
+# capture of the compress launches of an N=65536 factorization scaled by the box count
+# (x4) over this workload's 23 steps.
 COMPRESS_TRAFFIC_PER_STEP = 4 * 156.4e6 / 23
+# chosen form: factorization tolerance before refinement, refinement target and limit
+CHOSEN_TOL, IR_TOL, IR_MAXIT = 1e-6, 1e-10, 10
+SPHERE_NRHS = 64
+PREDICTOR_WEIGHTS = os.path.join(ROOT, "flam_b200", "predictor_weights.npz")
 
 
 def parse():
@@ -50,13 +63,16 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEF)
     ap.add_argument("--nrhs", type=int, default=NRHS_DEF)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-chosen", action="store_true", help="skip the chosen-form comparison")
+    ap.add_argument("--sphere-n", type=int, default=16384, help="points of the 3D sphere comparison")
     return ap.parse_args()
 
 
-def config(args, world):
-    return {"workload": f"rskelf star curve N={args.n} Beta(1/2,1/2)-clustered, occ {OCC}, tol {TOL:g}, "
+def config(args, world, n=None):
+    n = args.n if n is None else n
+    return {"workload": f"rskelf star curve N={n} Beta(1/2,1/2)-clustered, occ {OCC}, tol {TOL:g}, "
                         f"{args.nrhs} RHS, symm n, factor+solve per step",
-            "N_per_gpu": args.n, "nrhs": args.nrhs, "occ": OCC, "tol": TOL, "symm": "n",
+            "N_per_gpu": n, "nrhs": args.nrhs, "occ": OCC, "tol": TOL, "symm": "n",
             "parallelism": f"instances x{world} (one independent problem per rank)",
             "l2": "flushed between timed steps (256 MiB write); B (N x 256 FP64) is larger than L2"}
 
@@ -74,6 +90,16 @@ def cpu_sample(n, nrhs, seed=0):
     return time.perf_counter() - t0, n
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -86,8 +112,8 @@ def run_reference(args, rank, world):
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-           "config": config(args, 1),
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+           "config": config(args, 1, CPU_SAMPLE_N),
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "cpu": cpu_model(),
                             "sample": f"N={CPU_SAMPLE_N} instance of the same workload (NumPy/SciPy restatement of "
                                       f"the MATLAB reference, reference box order, {args.nrhs} RHS)"},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -153,16 +179,77 @@ def dgemm_peak(torch, dev):
     return best / 1e12
 
 
-def sampled_residual(x, w, X, B, rows):
-    """max over columns of ||A X - B|| / ||B|| on sampled rows, FP64 on the host."""
-    xs = x[:, rows]
-    d = xs[:, :, None] - x[:, None, :]
-    r2 = np.sum(d * d, axis=0)
-    with np.errstate(divide="ignore"):
-        K = -np.log(r2) / (4 * math.pi) * w[None, :]
-    K[np.arange(len(rows)), rows] = 1.0
-    R = K @ X - B[rows]
-    return float(np.max(np.linalg.norm(R, axis=0) / np.linalg.norm(B[rows], axis=0)))
+def relres(F, X, B):
+    """max over columns of ||B - A X|| / ||B||, FP64, with the library's on-the-fly matvec."""
+    import torch
+    R = torch.empty_like(B)
+    F.matvec_(X, R, B)
+    return float((R.norm(dim=0) / B.norm(dim=0)).max().item())
+
+
+def event_time(torch, stream, fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3, out
+
+
+# --------------------------------------------------------------------- chosen form
+def chosen_vs_plain(torch, fb, stream, name, Ad, xd, pxy, symm, Bd, plain_reps, chosen_reps, predictor, flush):
+    """One problem: plain FP64 at 1e-10 (factor + rskelf_sv) against the chosen form
+    (sketched factorization at CHOSEN_TOL + FP64 refinement to IR_TOL), both timed on the
+    device from the inputs in HBM, with their FP64 residuals."""
+    N = Bd.shape[0]
+    Xd = torch.empty_like(Bd)
+
+    def plain():
+        F = fb.rskelf(Ad, xd, OCC, TOL, pxy, dict(symm=symm, stream=stream.cuda_stream))
+        Xd.copy_(Bd)
+        F.sv_(Xd)
+        return F
+
+    copts = dict(symm=symm, stream=stream.cuda_stream, sketch=1, profile=True)
+    if predictor is not None:
+        copts.update(predictor=predictor, sketch_p=12)
+
+    def chosen():
+        F = fb.rskelf(Ad, xd, OCC, CHOSEN_TOL, pxy, copts)
+        _, it, rel = F.ir_sv_(Bd, Xd, IR_TOL, IR_MAXIT)
+        return F, it, rel
+
+    res = {}
+    tp = []
+    for rep in range(plain_reps + 1):          # one untimed warm-up
+        flush.fill_(float(rep))
+        t, F = event_time(torch, stream, plain)
+        if rep > 0 or plain_reps == 0:
+            tp.append(t)
+        if rep < plain_reps:
+            F.free()
+    res["plain"] = {"dofs": N / statistics.mean(tp), "ms": 1e3 * statistics.mean(tp), "steps": len(tp),
+                    "tol": TOL, "rel_residual_fp64": relres(F, Xd, Bd), "nfactor": F.info()["nfactor"]}
+    F.free()
+    tc = []
+    for rep in range(chosen_reps + 1):
+        flush.fill_(float(rep))
+        t, (F, it, rel) = event_time(torch, stream, chosen)
+        if rep > 0:
+            tc.append(t)
+        if rep < chosen_reps:
+            F.free()
+    prof = F.profile()
+    res["chosen"] = {"dofs": N / statistics.mean(tc), "ms": 1e3 * statistics.mean(tc), "steps": len(tc),
+                     "factor_tol": CHOSEN_TOL, "ir_tol": IR_TOL, "ir_steps": it,
+                     "rel_residual_fp64": relres(F, Xd, Bd), "rel_residual_reported": float(np.max(rel)),
+                     "sketched_boxes": prof["n_sketch"], "exact_redo_boxes": prof["n_sketch_redo"],
+                     "sketch_rows": prof["sketch_rows"], "rows_of_K": prof["sketch_rows_k"],
+                     "learned_widths": predictor is not None, "nfactor": F.info()["nfactor"]}
+    F.free()
+    res["ratio_chosen_over_plain"] = res["chosen"]["dofs"] / res["plain"]["dofs"]
+    res["problem"] = name
+    return res
 
 
 # --------------------------------------------------------------------- main
@@ -245,10 +332,8 @@ def main():
     t_step = max_over_ranks(statistics.mean(times))
     prof = F.profile()
     info = F.info()
-    # accuracy against FP64 on sampled rows (not timed)
-    rows = np.random.default_rng(7).choice(N, 64, replace=False)
-    Xh = Xd.cpu().numpy()
-    resid = sampled_residual(x, A.weights, Xh, B_host.numpy(), rows)
+    # accuracy against FP64: every column of the last step's solution (not timed)
+    resid = relres(F, Xd, Bd)
     F.free()
 
     # ---- end to end through the public API with pinned host buffers
@@ -311,8 +396,24 @@ def main():
             ts = [cpu_sample(CPU_SAMPLE_N, nrhs, seed=s)[0] for s in range(2)]
             tc = statistics.mean(ts)
             cpu = {"value": CPU_SAMPLE_N / tc, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                   "cpu": cpu_model(),
                    "sample": f"N={CPU_SAMPLE_N} instance of the same workload, oracle (NumPy/SciPy restatement of "
                              f"the reference, reference box order), {nrhs} RHS, mean of 2 runs"}
+        chosen = None
+        if not args.no_chosen:
+            pred = fb.Predictor.load(PREDICTOR_WEIGHTS) if os.path.exists(PREDICTOR_WEIGHTS) else None
+            chosen = {"note": "chosen = sketched (FP32/TF32 tensor-core) factorization at tol 1e-6 with learned "
+                              "sketch widths, refined in FP64 to 1e-10 (residual against the on-the-fly FP64 "
+                              "matvec); plain = FP64 exact ID at 1e-10 + rskelf_sv.  Both from inputs in HBM, "
+                              "CUDA events, one untimed warm-up each.",
+                      "star": chosen_vs_plain(torch, fb, stream, f"star N={N}, {nrhs} RHS (this workload)", Ad, xd,
+                                              pxy, "n", Bd, 3, 2, pred, flush)}
+            Ns = args.sphere_n
+            xs, As, ps = problems.sphere(Ns, p=256, seed=0)
+            xsd = torch.from_numpy(np.ascontiguousarray(xs.T)).to(dev).t()
+            Bs = torch.randn(Ns, SPHERE_NRHS, dtype=torch.float64, generator=gen).to(dev).t().contiguous().t()
+            chosen["sphere"] = chosen_vs_plain(torch, fb, stream, f"3D sphere N={Ns}, p=256, {SPHERE_NRHS} RHS",
+                                               As, xsd, ps, "n", Bs, 1, 2, pred, flush)
         h2d = N * 2 * 8 + N * 8 + N * nrhs * 8
         d2h = N * nrhs * 8
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -325,8 +426,10 @@ def main():
                "roofline": roofline,
                "cpu_baseline": cpu,
                "clocks": clocks,
-               "accuracy": {"rel_residual_fp64_sampled_rows": resid, "rows": 64,
-                            "note": "max over the 256 RHS of ||(A X - B)_rows|| / ||B_rows||, FP64 on the host"},
+               "accuracy": {"rel_residual_fp64": resid,
+                            "note": f"max over the {nrhs} RHS of ||B - A X|| / ||B||, every row, FP64 on-the-fly "
+                                    f"matvec (flam_matvec)"},
+               "chosen_form": chosen,
                "breakdown_ms": {"tree": info["t_tree"] * 1e3, "factor": info["t_factor"] * 1e3},
                "factor": {"nbox": info["nbox"], "nfactor": info["nfactor"], "levels": info["nstep"],
                           "device_bytes": info["bytes"]},

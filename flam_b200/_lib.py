@@ -24,7 +24,8 @@ EXPORTS = (
     "flam_level_stats", "flam_factor_free", "flam_workspace_release", "flam_profile", "flam_last_error", "flam_version",
     "flam_rskelf_cholmv", "flam_rskelf_cholsv", "flam_rskelf_logdet", "flam_partial_sizes", "flam_partial_export",
     "flam_rskelf_partial_sv", "flam_rskelf_partial_mv", "flam_factor_import", "flam_rskelf_diag",
-    "flam_matvec", "flam_rskelf_ir_sv",
+    "flam_matvec", "flam_rskelf_ir_sv", "flam_predictor_create", "flam_predictor_free", "flam_predictor_get",
+    "flam_predictor_set", "flam_predictor_train", "flam_predictor_eval", "flam_predictor_grad", "flam_rank_log",
 )
 
 # int fn(double* Y, int64_t n, int64_t nrhs, char trans, void* stream, void* ctx)
@@ -45,7 +46,7 @@ class FlamOpts(C.Structure):
     _fields_ = [("lvlmax", C.c_int), ("ext", C.c_void_p), ("Tmax", C.c_double), ("rrqr_iter", C.c_int64),
                 ("symm", C.c_char), ("stop", C.c_int), ("verb", C.c_int), ("stream", C.c_void_p),
                 ("profile", C.c_int), ("sketch", C.c_int), ("sketch_p", C.c_int), ("sketch_guard", C.c_int),
-                ("sketch_seed", C.c_uint), ("predictor", C.c_void_p)]
+                ("sketch_seed", C.c_uint), ("predictor", C.c_void_p), ("rank_log", C.c_int)]
 
 
 class FlamInfo(C.Structure):
@@ -58,7 +59,8 @@ class FlamProf(C.Structure):
     _fields_ = [("launches", C.c_int64), ("n_compress", C.c_int64), ("n_elim", C.c_int64), ("n_sweep", C.c_int64),
                 ("t_compress", C.c_double), ("t_elim", C.c_double), ("t_sweep", C.c_double),
                 ("flop_compress", C.c_double), ("flop_elim", C.c_double), ("flop_sweep", C.c_double),
-                ("byte_sweep", C.c_double), ("n_sketch", C.c_int64), ("n_sketch_redo", C.c_int64)]
+                ("byte_sweep", C.c_double), ("n_sketch", C.c_int64), ("n_sketch_redo", C.c_int64),
+                ("sketch_rows", C.c_int64), ("sketch_rows_k", C.c_int64), ("id_rows", C.c_int64)]
 
 
 class FlamError(RuntimeError):
@@ -114,6 +116,23 @@ def lib():
     L.flam_rskelf_ir_sv.argtypes = [P, P, C.c_int64, P, C.c_int64, C.c_int64, C.c_double, C.c_int,
                                     C.POINTER(C.c_int), dp]
     L.flam_rskelf_ir_sv.restype = C.c_int
+    fp = C.POINTER(C.c_float)
+    L.flam_predictor_create.argtypes = [C.c_uint64, C.POINTER(P)]
+    L.flam_predictor_create.restype = C.c_int
+    L.flam_predictor_free.argtypes = [P]
+    L.flam_predictor_free.restype = None
+    L.flam_predictor_get.argtypes = [P, fp]
+    L.flam_predictor_get.restype = C.c_int
+    L.flam_predictor_set.argtypes = [P, fp]
+    L.flam_predictor_set.restype = C.c_int
+    L.flam_predictor_train.argtypes = [P, fp, fp, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, fp]
+    L.flam_predictor_train.restype = C.c_int
+    L.flam_predictor_eval.argtypes = [P, fp, C.c_int64, fp]
+    L.flam_predictor_eval.restype = C.c_int
+    L.flam_predictor_grad.argtypes = [P, fp, fp, C.c_int64, fp, fp]
+    L.flam_predictor_grad.restype = C.c_int
+    L.flam_rank_log.argtypes = [P, C.POINTER(C.c_int64), fp, fp]
+    L.flam_rank_log.restype = C.c_int
     L.flam_rskelf_diag.argtypes = [P, C.c_int, P]
     L.flam_rskelf_diag.restype = C.c_int
     L.flam_rskelf_logdet.argtypes = [P, dp, dp]

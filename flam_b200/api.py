@@ -27,7 +27,7 @@ from . import _lib
 from .registry import Kernel, Proxy
 
 _OPT_KEYS = {"lvlmax", "ext", "Tmax", "rrqr_iter", "symm", "stop", "verb", "stream", "profile", "sketch", "sketch_p",
-             "sketch_guard", "sketch_seed", "predictor"}
+             "sketch_guard", "sketch_seed", "predictor", "rank_log"}
 
 
 def _c_opts(opts):
@@ -64,6 +64,8 @@ def _c_opts(opts):
             o.sketch_seed = int(v) & 0xFFFFFFFF
         elif k == "predictor":
             o.predictor = None if v is None else (v.handle if hasattr(v, "handle") else v)
+        elif k == "rank_log":
+            o.rank_log = int(bool(v))
     return o, keep
 
 
@@ -270,6 +272,17 @@ class Factor:
                                                 int(max_iter), C.byref(it),
                                                 rel.ctypes.data_as(C.POINTER(C.c_double))))
         return X, it.value, rel[:nrhs]
+
+    def rank_log(self):
+        """(features, k/n) of every compressed box of a factorization made with opts rank_log."""
+        L = _lib.lib()
+        cnt = C.c_int64()
+        _lib.check(L.flam_rank_log(self._h, C.byref(cnt), None, None))
+        X = np.zeros((max(cnt.value, 1), 16), np.float32)
+        y = np.zeros(max(cnt.value, 1), np.float32)
+        fp = C.POINTER(C.c_float)
+        _lib.check(L.flam_rank_log(self._h, C.byref(cnt), X.ctypes.data_as(fp), y.ctypes.data_as(fp)))
+        return X[:cnt.value], y[:cnt.value]
 
     # ------------------------------------------------------- partial factorization
     def partial_info(self, inst=0):
@@ -552,3 +565,80 @@ def id(A, rank_or_tol, Tmax=2.0, rrqr_iter=math.inf):  # noqa: A001 - the refere
 def hypoct_perm(T):
     """P = hypoct_perm(T) for a handle returned by :func:`hypoct` or :func:`rskelf`."""
     return T.perm(0)
+
+
+class Predictor:
+    """Learned rank predictor (flam_predictor): a BF16 MLP 16 -> 128 -> 128 -> 1 trained and
+    evaluated on the GPU by the library's own kernels.  Pass it as ``opts["predictor"]``
+    together with ``opts["sketch"] = 1`` to size each box's sketch from its prediction."""
+
+    NPARAM = 18817
+    NFEAT = 16
+
+    def __init__(self, seed=0, weights=None):
+        h = C.c_void_p()
+        _lib.check(_lib.lib().flam_predictor_create(int(seed), C.byref(h)))
+        self.handle = h.value
+        self._free = _lib.lib().flam_predictor_free
+        if weights is not None:
+            self.set_weights(weights)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            self._free(h)
+            self.handle = None
+
+    @staticmethod
+    def _f32(a, shape=None):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        if shape is not None and a.shape != shape:
+            raise _lib.FlamError(1, f"FLAM:predictor:invalidArg: expected shape {shape}, got {a.shape}")
+        return a
+
+    def weights(self):
+        w = np.zeros(self.NPARAM, np.float32)
+        _lib.check(_lib.lib().flam_predictor_get(self.handle, w.ctypes.data_as(C.POINTER(C.c_float))))
+        return w
+
+    def set_weights(self, w):
+        w = self._f32(w, (self.NPARAM,))
+        _lib.check(_lib.lib().flam_predictor_set(self.handle, w.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def train(self, X, y, epochs=50, batch=256, lr=2e-3, seed=0):
+        X = self._f32(X)
+        y = self._f32(y)
+        if X.ndim != 2 or X.shape[1] != self.NFEAT or y.shape != (X.shape[0],):
+            raise _lib.FlamError(1, "FLAM:predictor:invalidArg: X must be n x 16 and y of length n")
+        loss = C.c_float()
+        fp = C.POINTER(C.c_float)
+        _lib.check(_lib.lib().flam_predictor_train(self.handle, X.ctypes.data_as(fp), y.ctypes.data_as(fp),
+                                                   X.shape[0], int(epochs), int(batch), float(lr), int(seed),
+                                                   C.byref(loss)))
+        return loss.value
+
+    def predict(self, X):
+        X = self._f32(X)
+        out = np.zeros(max(X.shape[0], 1), np.float32)
+        fp = C.POINTER(C.c_float)
+        _lib.check(_lib.lib().flam_predictor_eval(self.handle, X.ctypes.data_as(fp), X.shape[0],
+                                                  out.ctypes.data_as(fp)))
+        return out[:X.shape[0]]
+
+    def grad(self, X, y):
+        """(mean squared error, its gradient) of one forward/backward pass on the GPU."""
+        X = self._f32(X)
+        y = self._f32(y)
+        g = np.zeros(self.NPARAM, np.float32)
+        loss = C.c_float()
+        fp = C.POINTER(C.c_float)
+        _lib.check(_lib.lib().flam_predictor_grad(self.handle, X.ctypes.data_as(fp), y.ctypes.data_as(fp),
+                                                  X.shape[0], C.byref(loss), g.ctypes.data_as(fp)))
+        return loss.value, g
+
+    def save(self, path):
+        np.savez_compressed(path, w=self.weights())
+
+    @classmethod
+    def load(cls, path):
+        return cls(weights=np.load(path)["w"])

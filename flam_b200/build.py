@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libflam_b200.so")
-SOURCES = ["scan.cu", "tree.cu", "compress.cu", "compress_tc.cu", "eliminate.cu", "sweep.cu", "logdet.cu", "diag.cu", "capi.cu", "noalloc.cu", "matvec.cu", "sketch.cu"]
+SOURCES = ["scan.cu", "tree.cu", "compress.cu", "compress_tc.cu", "eliminate.cu", "sweep.cu", "logdet.cu", "diag.cu", "capi.cu", "noalloc.cu", "matvec.cu", "sketch.cu", "predictor.cu", "cpqr_wide.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]

@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "matvec.cuh"
+#include "predictor.cuh"
 #include "scan.cuh"
 #include "sketch.cuh"
 #include "tree.cuh"
@@ -180,8 +181,10 @@ struct Workspace {
   // sketched compression: row sketches, their tasks, rows of K per box, boxes redone exactly
   DBuf<double> ypool;
   DBuf<SketchTask> sktask;
-  DBuf<CompressTask> skfilt, redo_task;
+  DBuf<CompressTask> skfilt, redo_task, wtask;
   DBuf<int32_t> mrows, redo_idx;
+  DBuf<CompressTask> ftask;
+  DBuf<float> feat, fyhat;
   DBuf<double> irB, irX, irR, irW, colsq;
   cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
   // side streams for the independent launches of one step (the kernel shapes of a
@@ -267,8 +270,12 @@ struct Workspace {
     sktask.release(s);
     skfilt.release(s);
     redo_task.release(s);
+    wtask.release(s);
     mrows.release(s);
     redo_idx.release(s);
+    ftask.release(s);
+    feat.release(s);
+    fyhat.release(s);
     cpool.release(s);
     permpool.release(s);
     status.release(s);
@@ -338,6 +345,7 @@ struct flam_factor {
   int64_t Sn_tot = 0;
   double t_tree = 0, t_factor = 0;
   int64_t warn = 0;
+  std::vector<float> rlog_X, rlog_y;   // opts.rank_log: features and k/n of every compressed box
   bool profile = false;
   mutable flam_prof prof{};
   mutable cudaEvent_t pend[2] = {nullptr, nullptr};   // sweep timing not yet read
@@ -370,6 +378,16 @@ struct flam_factor {
     Si_dev.release(st);
     for (auto& q : steps) q.fac.release(st);
     cudaStreamSynchronize(st);
+  }
+};
+
+struct flam_predictor {
+  int dev = 0;
+  DBuf<float> w, m, v, grad, scal, X, y, yhat;
+  int step = 0;
+  ~flam_predictor() {
+    for (auto* b : {&w, &m, &v, &grad, &scal, &X, &y, &yhat}) b->release(nullptr);
+    cudaStreamSynchronize(nullptr);
   }
 };
 
@@ -979,7 +997,46 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     }();
     // sketched compression (opts.sketch): boxes of at most kSketchMaxN points whose block
     // has more rows than the sketch take Y = Omega K (w rows) and an ID of Y
+    // box features (rank predictor, rank log): from the slf lists, gathered here already
+    const flam_predictor* pred = o.sketch ? static_cast<const flam_predictor*>(o.predictor) : nullptr;
     std::vector<int> pred_k;   // per box: the rank predictor's estimate (empty: no predictor)
+    std::vector<CompressTask> ftv;
+    if (pred || o.rank_log) {
+      ftv.resize(nb);
+      for (int q = 0; q < nb; ++q) {
+        const int32_t b = boxes[q];
+        const int i = F.binst[b];
+        CompressTask& u = ftv[q];
+        u.slf_off = slf_off[q];
+        u.n = (int32_t)nslf[q];
+        u.ncand = (int32_t)ncand[q];
+        u.inst = i;
+        u.box = b;
+        u.depth = F.depth[b];
+        u.flags = (F.depth[b] > 2 && F.iph[i].pkind != P_NONE) ? 1 : 0;
+        for (int c = 0; c < kMaxDim; ++c) {
+          u.ctr[c] = c < F.d ? F.ctr[(size_t)b * F.d + c] : 0.0;
+          u.l[c] = c < F.d ? F.lsz[(size_t)b * F.d + c] : 0.0;
+        }
+      }
+      segs.upload(sg, s);
+      launch_gather_ids(F.ipool.p, F.ipool.p, segs.p, (int)sg.size(), s);
+      ws.ftask.upload(ftv, s);
+      ws.feat.ensure((int64_t)nb * kPredFeatures, s);
+      launch_box_features(ws.ftask.p, nb, F.ipool.p, P, rel_tol > 0 ? (float)-std::log10(rel_tol) : 16.f, ws.feat.p,
+                          s);
+      F.prof.launches += 2;
+      if (pred) {
+        if (pred->dev != F.dev) fail(FLAM_ERR_ARG, "FLAM:gpu:predictorDevice: the predictor lives on another device");
+        ws.fyhat.ensure(nb, s);
+        launch_mlp(ws.feat.p, nullptr, nb, pred->w.p, ws.fyhat.p, nullptr, nullptr, 0.f, 0, s);
+        F.prof.launches += 1;
+        CK(cudaGetLastError());
+        auto yh = download(ws.fyhat.p, nb, s);
+        pred_k.resize(nb);
+        for (int q = 0; q < nb; ++q) pred_k[q] = (int)std::ceil((double)yh[q] * (double)nslf[q]);
+      }
+    }
     std::vector<int> skw(nb, 0);
     std::vector<int64_t> yoff(nb, -1);
     int64_t ytop = 0;
@@ -1028,6 +1085,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       t.perm_off = ptop;
       ptop += nslf[q];
       t.out_idx = q;
+      t.depth = F.depth[b];
       // work matrices: shared memory when they fit, else a per-box slot of global scratch
       // shared by the compress and elimination kernels of this step
       const int n = (int)nslf[q];
@@ -1078,7 +1136,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     cts.reserve(nb * 3);
     // sketched boxes: their filter and sketch tasks, and the ID of Y in place of K's rows
     std::vector<SketchTask> skt;
-    std::vector<CompressTask> skf;
+    std::vector<CompressTask> skf, wts;
     std::vector<int> sk_of(nb, -1);
     const int sk_guard = std::max(0, o.sketch_guard);
     for (int q : ord) {
@@ -1103,7 +1161,19 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         u.l[c] = c0.l[c];
       }
       sk_of[q] = (int)skt.size();
-      skt.push_back(u);
+      // CTAs of the box: all of it in one when it fits 256 x 256, else 128 columns of K by
+      // up to 512 rows of Y each
+      const bool one = u.n <= kSketchCtaCols && u.w <= kSketchCtaCols;
+      const int cstep = one ? u.n : 128, jstep = one ? u.w : kSketchCtaRows;
+      for (int c0i = 0; c0i < u.n; c0i += cstep)
+        for (int j0i = 0; j0i < u.w; j0i += jstep) {
+          SketchTask v2 = u;
+          v2.col0 = c0i;
+          v2.ncol = std::min(cstep, u.n - c0i);
+          v2.j0 = j0i;
+          v2.nw = std::min(jstep, u.w - j0i);
+          skt.push_back(v2);
+        }
       skf.push_back(c0);
       CompressTask v = c0;
       v.flags = 0;
@@ -1111,7 +1181,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       v.ax_off = yoff[q];
       v.ax_rows = skw[q];
       v.ax_guard = sk_guard;
-      cts.push_back(v);
+      if (v.n > kTcMaxN)
+        wts.push_back(v);   // wider than a thread per column: the wide pivoted QR
+      else
+        cts.push_back(v);
     }
     std::vector<int> seg{(int)cts.size()};
     std::vector<int> sord;
@@ -1232,10 +1305,17 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       sa.seed = o.sketch_seed;
       sa.status = status.p;
       size_t smx = 0;
-      for (const SketchTask& u : skt) smx = std::max(smx, sketch_smem_bytes(u.n, u.w));
+      for (const SketchTask& u : skt) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
       launch_sketch(sa, (int)skt.size(), smx, s);
       F.prof.launches += 2;
-      F.prof.n_sketch += (int64_t)skt.size();
+      if (!wts.empty()) {
+        ws.wtask.upload(wts, s);
+        CompressArgs cw = ca;
+        cw.tasks = ws.wtask.p;
+        launch_cpqr_wide(cw, (int)wts.size(), s);
+        F.prof.launches += 1;
+      }
+      F.prof.n_sketch += (int64_t)skf.size();
     }
     launch_segment(0, seg[0]);
     if (seg.size() > 1) {
@@ -1249,6 +1329,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     CK(cudaGetLastError());
     if (prof) CK(cudaEventRecord(pe[1], s));
     auto co = download(cout.p, nb, s);
+    std::vector<char> redone(nb, 0);
     if (!skt.empty()) {
       // posterior check of the sketched IDs: a box whose rank came within sketch_guard of
       // its sketch rows is redone with the exact ID of K (from the pull-up order, with the
@@ -1258,7 +1339,11 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         if (skw[q] > 0 && (co[q].status & ST_ID_CHECK)) redo.push_back(q);
       auto mr = download(ws.mrows.p, nb, s);
       for (int q = 0; q < nb; ++q)
-        if (skw[q] > 0) co[q].m = mr[q];   // rows of K, for the work accounting
+        if (skw[q] > 0) {
+          co[q].m = mr[q];   // rows of K, for the work accounting
+          F.prof.sketch_rows += skw[q];
+          F.prof.sketch_rows_k += mr[q];
+        }
       if (!redo.empty()) {
         auto mf = download(ws.mfilt.p, nb, s);
         std::vector<int32_t> ridx;
@@ -1287,7 +1372,10 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           }
           CompressArgs cr = ca;
           cr.tasks = ws.redo_task.p + b0;
-          launch_compress_tc(cr, (int)(b1 - b0), key / 1000, (key / 10) % 100, key % 10, sm, s);
+          if (key == 0)   // n > kTcMaxN: the per-column kernel
+            launch_compress(cr, (int)(b1 - b0), 0, s);
+          else
+            launch_compress_tc(cr, (int)(b1 - b0), key / 1000, (key / 10) % 100, key % 10, sm, s);
           F.prof.launches += 1;
           b0 = b1;
         }
@@ -1295,10 +1383,24 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         F.prof.launches += 1;
         F.prof.n_sketch_redo += (int64_t)redo.size();
         auto co2 = download(cout.p, nb, s);
-        for (int q : redo) co[q] = co2[q];
+        for (int q : redo) {
+          co[q] = co2[q];
+          redone[q] = 1;
+        }
       }
     }
 
+    for (int q = 0; q < nb; ++q)   // a redone box folded its sketch and then K
+      F.prof.id_rows += skw[q] > 0 ? skw[q] + (redone[q] ? co[q].m : 0) : co[q].m;
+    if (o.rank_log) {   // features and k/n of every box that was compressed (n > 0)
+      auto fv = download(ws.feat.p, (int64_t)nb * kPredFeatures, s);
+      for (int q = 0; q < nb; ++q) {
+        if (nslf[q] == 0) continue;
+        F.rlog_X.insert(F.rlog_X.end(), fv.begin() + (size_t)q * kPredFeatures,
+                        fv.begin() + (size_t)(q + 1) * kPredFeatures);
+        F.rlog_y.push_back((float)co[q].k / (float)nslf[q]);
+      }
+    }
     // ---- elimination plan
     std::vector<ElimTask> et(nb);
     std::vector<FacDesc> fd;
@@ -1365,13 +1467,25 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     F.ppool.n = ppool_top;
     mpool[cur].ensure(std::max<int64_t>(mtop, 1), es0);
     // boxes whose work matrix is in global memory go to the blocked kernel: upload them last
+    // [n <= kSmemN: shared-memory kernel | larger: one CTA per box | r >= kHugeR: grid-wide]
+    auto huge = [](const ElimTask& e) { return e.n > kSmemN && e.n - e.k >= kHugeR; };
     std::vector<ElimTask> ets;
     ets.reserve(nb);
     for (const ElimTask& e : et)
       if (e.n <= kSmemN) ets.push_back(e);
     const int nsmall_e = (int)ets.size();
     for (const ElimTask& e : et)
-      if (e.n > kSmemN) ets.push_back(e);
+      if (e.n > kSmemN && !huge(e)) ets.push_back(e);
+    const int nbig_e = (int)ets.size() - nsmall_e;
+    int hn = 0, hk = 0, hr = 0;
+    for (const ElimTask& e : et)
+      if (huge(e)) {
+        ets.push_back(e);
+        hn = std::max(hn, e.n);
+        hk = std::max(hk, e.k);
+        hr = std::max(hr, e.n - e.k);
+      }
+    const int nhuge_e = (int)ets.size() - nsmall_e - nbig_e;
     etask.upload(ets, es0);
     chb.upload(ch, es0);
     ElimArgs ea{};
@@ -1409,9 +1523,15 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       ElimArgs eb = ea;
       eb.tasks = etask.p + nsmall_e;
       int rbig = 0;   // the largest redundant block among the big boxes: its LU panel height
-      for (int q = nsmall_e; q < nb; ++q) rbig = std::max(rbig, ets[q].n - ets[q].k);
+      for (int q = nsmall_e; q < nsmall_e + nbig_e; ++q) rbig = std::max(rbig, ets[q].n - ets[q].k);
       eb.pan_rows = rbig <= elim_pan_rows_max() ? rbig : 0;
-      launch_eliminate(eb, 0, nb - nsmall_e, 0, es1);
+      if (nbig_e > 0) launch_eliminate(eb, 0, nbig_e, 0, es1);
+      if (nhuge_e > 0) {
+        ElimArgs eh = ea;
+        eh.tasks = etask.p + nsmall_e + nbig_e;
+        launch_eliminate_huge(eh, nhuge_e, hn, hk, hr, es1);
+        F.prof.launches += elim_huge_launches(hr, hk, F.symm == 'p') - 1;
+      }
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ws.edone[par][0], es0));
@@ -2141,6 +2261,7 @@ void flam_opts_default(flam_opts* o) {
   o->sketch_guard = 2;
   o->sketch_seed = 0x5eed1234u;
   o->predictor = nullptr;
+  o->rank_log = 0;
 }
 
 flam_status flam_rskelf(const double* x, int d, int64_t N, const flam_kernel* A, double occ, double rank_or_tol,
@@ -2287,6 +2408,170 @@ flam_status flam_matvec(const flam_factor* F, const double* X, int64_t ldx, int6
 flam_status flam_rskelf_ir_sv(const flam_factor* F, const double* B, int64_t ldb, double* X, int64_t ldx, int64_t nrhs,
                               double ir_tol, int max_iter, int* iters, double* relres) {
   return guard([&] { return ir_solve(F, B, ldb, X, ldx, nrhs, ir_tol, max_iter, iters, relres); });
+}
+
+// ---------------------------------------------------------------- rank predictor
+flam_status flam_predictor_create(uint64_t seed, flam_predictor** P) {
+  return guard([&] {
+    if (!P) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: NULL output");
+    *P = nullptr;
+    std::unique_ptr<flam_predictor> p(new flam_predictor());
+    CK(cudaGetDevice(&p->dev));
+    // He initialisation (Box-Muller on a splitmix64 stream), zero biases
+    std::vector<float> w(FLAM_PREDICTOR_NPARAM, 0.f);
+    uint64_t st = seed + 0x9E3779B97F4A7C15ull;
+    auto next = [&]() {
+      uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      return ((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto gauss = [&]() {
+      const double u1 = std::max(next(), 1e-300), u2 = next();
+      return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    };
+    const int nin = FLAM_PREDICTOR_NFEAT, nh = 128;
+    for (int e = 0; e < nh * nin; ++e) w[e] = (float)(gauss() * std::sqrt(2.0 / nin));
+    const int w2 = nh * nin + nh;
+    for (int e = 0; e < nh * nh; ++e) w[w2 + e] = (float)(gauss() * std::sqrt(2.0 / nh));
+    const int w3 = w2 + nh * nh + nh;
+    for (int e = 0; e < nh; ++e) w[w3 + e] = (float)(gauss() * std::sqrt(1.0 / nh));
+    p->w.upload(w, nullptr);
+    std::vector<float> z(FLAM_PREDICTOR_NPARAM, 0.f);
+    p->m.upload(z, nullptr);
+    p->v.upload(z, nullptr);
+    p->grad.upload(z, nullptr);
+    p->scal.ensure(4, nullptr);
+    CK(cudaStreamSynchronize(nullptr));
+    *P = p.release();
+    return FLAM_OK;
+  });
+}
+
+void flam_predictor_free(flam_predictor* P) { delete P; }
+
+flam_status flam_predictor_get(const flam_predictor* P, float* w) {
+  return guard([&] {
+    if (!P || !w) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: NULL argument");
+    CK(cudaMemcpy(w, P->w.p, sizeof(float) * FLAM_PREDICTOR_NPARAM, cudaMemcpyDefault));
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_predictor_set(flam_predictor* P, const float* w) {
+  return guard([&] {
+    if (!P || !w) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: NULL argument");
+    CK(cudaMemcpy(P->w.p, w, sizeof(float) * FLAM_PREDICTOR_NPARAM, cudaMemcpyDefault));
+    CK(cudaMemset(P->m.p, 0, sizeof(float) * FLAM_PREDICTOR_NPARAM));
+    CK(cudaMemset(P->v.p, 0, sizeof(float) * FLAM_PREDICTOR_NPARAM));
+    P->step = 0;
+    return FLAM_OK;
+  });
+}
+
+namespace {
+void pred_inputs(flam_predictor* P, const float* X, const float* y, int64_t nsamp) {
+  if (nsamp < 0) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: nsamp < 0");
+  if (nsamp == 0) return;
+  if (!X) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: X is NULL");
+  P->X.ensure(nsamp * FLAM_PREDICTOR_NFEAT, nullptr);
+  CK(cudaMemcpy(P->X.p, X, sizeof(float) * nsamp * FLAM_PREDICTOR_NFEAT, cudaMemcpyDefault));
+  if (y) {
+    P->y.ensure(nsamp, nullptr);
+    CK(cudaMemcpy(P->y.p, y, sizeof(float) * nsamp, cudaMemcpyDefault));
+  }
+}
+}  // namespace
+
+flam_status flam_predictor_train(flam_predictor* P, const float* X, const float* y, int64_t nsamp, int epochs,
+                                 int batch, float lr, uint64_t seed, float* loss) {
+  return guard([&] {
+    if (!P || !y) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: NULL argument");
+    if (epochs < 0 || batch < 1 || !(lr > 0)) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: epochs, batch or lr");
+    if (nsamp == 0) return FLAM_OK;
+    // shuffled copies per epoch (the samples are small: 68 bytes each)
+    std::vector<float> hx((size_t)nsamp * FLAM_PREDICTOR_NFEAT), hy((size_t)nsamp);
+    CK(cudaMemcpy(hx.data(), X, sizeof(float) * hx.size(), cudaMemcpyDefault));
+    CK(cudaMemcpy(hy.data(), y, sizeof(float) * hy.size(), cudaMemcpyDefault));
+    std::vector<int64_t> idx((size_t)nsamp);
+    uint64_t st = seed * 0x2545F4914F6CDD1Dull + 1;
+    auto rnd = [&]() {
+      st ^= st >> 12;
+      st ^= st << 25;
+      st ^= st >> 27;
+      return st * 0x2545F4914F6CDD1Dull;
+    };
+    std::vector<float> sx(hx.size()), sy(hy.size());
+    double last = 0;
+    for (int ep = 0; ep < epochs; ++ep) {
+      for (int64_t i = 0; i < nsamp; ++i) idx[i] = i;
+      for (int64_t i = nsamp - 1; i > 0; --i) std::swap(idx[i], idx[rnd() % (uint64_t)(i + 1)]);
+      for (int64_t i = 0; i < nsamp; ++i) {
+        std::memcpy(&sx[(size_t)i * FLAM_PREDICTOR_NFEAT], &hx[(size_t)idx[i] * FLAM_PREDICTOR_NFEAT],
+                    sizeof(float) * FLAM_PREDICTOR_NFEAT);
+        sy[i] = hy[idx[i]];
+      }
+      pred_inputs(P, sx.data(), sy.data(), nsamp);
+      CK(cudaMemset(P->scal.p, 0, sizeof(float)));
+      for (int64_t b0 = 0; b0 < nsamp; b0 += batch) {
+        const int64_t nbat = std::min<int64_t>(batch, nsamp - b0);
+        launch_mlp(P->X.p + b0 * FLAM_PREDICTOR_NFEAT, P->y.p + b0, nbat, P->w.p, nullptr, P->grad.p, P->scal.p,
+                   1.f / (float)nbat, 1, nullptr);
+        launch_adam(P->w.p, P->m.p, P->v.p, P->grad.p, lr, ++P->step, nullptr);
+      }
+      CK(cudaGetLastError());
+      float sse = 0;
+      CK(cudaMemcpy(&sse, P->scal.p, sizeof(float), cudaMemcpyDeviceToHost));
+      last = sse / (double)nsamp;
+    }
+    if (loss) *loss = (float)last;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_predictor_eval(const flam_predictor* P, const float* X, int64_t nsamp, float* yhat) {
+  return guard([&] {
+    if (!P || !yhat) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: NULL argument");
+    auto* Q = const_cast<flam_predictor*>(P);
+    pred_inputs(Q, X, nullptr, nsamp);
+    if (nsamp == 0) return FLAM_OK;
+    Q->yhat.ensure(nsamp, nullptr);
+    launch_mlp(Q->X.p, nullptr, nsamp, Q->w.p, Q->yhat.p, nullptr, nullptr, 0.f, 0, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(yhat, Q->yhat.p, sizeof(float) * nsamp, cudaMemcpyDefault));
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_predictor_grad(const flam_predictor* P, const float* X, const float* y, int64_t nsamp, float* loss,
+                                float* grad) {
+  return guard([&] {
+    if (!P || !y || !grad || nsamp < 1) fail(FLAM_ERR_ARG, "FLAM:predictor:invalidArg: NULL argument or no samples");
+    auto* Q = const_cast<flam_predictor*>(P);
+    pred_inputs(Q, X, y, nsamp);
+    DBuf<float> g;
+    g.ensure(FLAM_PREDICTOR_NPARAM + 1, nullptr);
+    CK(cudaMemset(g.p, 0, sizeof(float) * (FLAM_PREDICTOR_NPARAM + 1)));
+    launch_mlp(Q->X.p, Q->y.p, nsamp, Q->w.p, nullptr, g.p, g.p + FLAM_PREDICTOR_NPARAM, 1.f / (float)nsamp, 1,
+               nullptr);
+    CK(cudaGetLastError());
+    std::vector<float> h(FLAM_PREDICTOR_NPARAM + 1);
+    CK(cudaMemcpy(h.data(), g.p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost));
+    g.release(nullptr);
+    std::copy(h.begin(), h.begin() + FLAM_PREDICTOR_NPARAM, grad);
+    if (loss) *loss = h[FLAM_PREDICTOR_NPARAM] / (float)nsamp;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_rank_log(const flam_factor* F, int64_t* count, float* X, float* y) {
+  return guard([&] {
+    if (!F || !count) fail(FLAM_ERR_ARG, "FLAM:rank_log:invalidArg: NULL argument");
+    *count = (int64_t)F->rlog_y.size();
+    if (X) std::copy(F->rlog_X.begin(), F->rlog_X.end(), X);
+    if (y) std::copy(F->rlog_y.begin(), F->rlog_y.end(), y);
+    return FLAM_OK;
+  });
 }
 
 flam_status flam_rskelf_sv(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, char trans) {

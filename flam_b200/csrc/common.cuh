@@ -74,7 +74,7 @@ struct CompressTask {
   // the rest of the ID.  Modes 1-3 read the filtered candidate count from mfilt.
   int32_t mode;
   int32_t part, nparts;
-  int32_t pad_;
+  int32_t depth;     // tree level of the box (box features of the rank predictor)
   int64_t rsrc_off;
   // Sketched form: with ax_rows > 0 the rows of the block are the explicit ax_rows x n
   // matrix (column-major, leading dimension ax_rows) at ax_off of the sketch pool -- the

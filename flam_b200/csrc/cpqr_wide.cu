@@ -1,0 +1,275 @@
+// ID of a short, wide explicit matrix: the row sketch Y (w x n, w <= 1024 rows) of a box
+// with more points than the thread-per-column compression takes (n > 1024).
+//
+// Same decisions as the other compression kernels (core/id.m:102-114 on Y): column-
+// pivoted Householder QR with LAPACK xLAQP2's rule (first maximum of the partial column
+// norms, sqrt(eps) recomputation threshold), stopping at the first |R(i,i)| <=
+// tol |R(0,0)| in tolerance mode, the rank, T = R11 \ R12 and, when some |T| > Tmax, the
+// RRQR refinement of id.m:116-236 (rrqr.cuh).  One CTA per box; Y is updated in place
+// in global memory (L2-resident), a warp per column for the reflector products (lanes
+// over rows: coalesced), the reflector in shared memory.  T is solved column by column
+// by one warp each, the right-hand side held in registers across the lanes.
+#include <cmath>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "rrqr.cuh"
+
+namespace flam {
+namespace {
+
+constexpr int kWThreads = 512;
+constexpr int kWWarps = kWThreads / 32;
+constexpr int kWMaxRows = 1024;
+
+struct WAm {
+  double v;
+  int i;
+};
+__device__ __forceinline__ WAm wbetter(WAm a, WAm b) {
+  if (b.v > a.v || (b.v == a.v && b.i < a.i)) return b;
+  return a;
+}
+
+__global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
+  __shared__ double vbuf[kWMaxRows];
+  __shared__ double red[kWWarps];
+  __shared__ WAm ram[kWWarps];
+  __shared__ int s_k, s_ktol, s_niter, s_cap, s_need, s_pvt, s_stop;
+  __shared__ double s_tau, s_r00;
+  const CompressTask t = a.tasks[blockIdx.x];
+  const int n = t.n, w = t.ax_rows;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  CompressOut* out = a.out + t.out_idx;
+  double* Y = const_cast<double*>(a.ypool) + t.ax_off;   // w x n, ld w
+  auto y = [&](int r, int c) -> double& { return Y[r + (int64_t)c * w]; };
+  double* sc = a.scratch + t.scr_off;
+  double* vn1 = sc;
+  double* vn2 = vn1 + n;
+  double* aux = vn2 + n;                                  // 6n: RRQR norms and work
+  int* jpvt = reinterpret_cast<int*>(aux + 6 * (int64_t)n);
+  int64_t* slf = a.ipool + t.slf_off;
+  if (n == 0 || w > kWMaxRows) {
+    if (tid == 0) *out = CompressOut{0, 0, 0, n == 0 ? 0 : (int)ST_ID_CHECK};
+    return;
+  }
+  const int mn = min(w, n);
+  // column norms
+  for (int c = wid; c < n; c += kWWarps) {
+    double s = 0.0;
+    for (int r = lane; r < w; r += 32) s += y(r, c) * y(r, c);
+    s = warp_sum(s);
+    if (lane == 0) {
+      vn1[c] = vn2[c] = sqrt(s);
+      jpvt[c] = c;
+    }
+  }
+  if (tid == 0) s_stop = mn;
+  __syncthreads();
+  const double tol3z = 1.0536712127723509e-08;   // sqrt(2^-53)
+  const bool stop_early = a.kmax == 0;
+  for (int i = 0; i < mn; ++i) {
+    // pivot: the first maximum of the partial norms over columns i..n-1
+    WAm am{-1.0, n};
+    for (int c = i + tid; c < n; c += kWThreads) am = wbetter(am, WAm{vn1[c], c});
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      WAm b{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+      am = wbetter(am, b);
+    }
+    if (lane == 0) ram[wid] = am;
+    __syncthreads();
+    if (tid == 0) {
+      WAm bm = ram[0];
+      for (int q = 1; q < kWWarps; ++q) bm = wbetter(bm, ram[q]);
+      s_pvt = (bm.i >= i && bm.i < n) ? bm.i : i;
+    }
+    __syncthreads();
+    const int pvt = s_pvt;
+    // swap columns i and pvt; gather the reflector's rows into shared memory
+    double s = 0.0;
+    for (int r = tid; r < w; r += kWThreads) {
+      const double v = y(r, pvt);
+      if (pvt != i) {
+        y(r, pvt) = y(r, i);
+        y(r, i) = v;
+      }
+      vbuf[r] = v;
+      if (r > i) s += v * v;
+    }
+    if (tid == 0 && pvt != i) {
+      const int tj = jpvt[pvt];
+      jpvt[pvt] = jpvt[i];
+      jpvt[i] = tj;
+      vn1[pvt] = vn1[i];
+      vn2[pvt] = vn2[i];
+    }
+    s = warp_sum(s);
+    if (lane == 0) red[wid] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double ss = 0.0;
+      for (int q = 0; q < kWWarps; ++q) ss += red[q];
+      const double al = vbuf[i];
+      const double dii = ss != 0.0 ? -copysign(hypot(al, sqrt(ss)), al) : al;
+      if (i == 0) s_r00 = fabs(dii);
+      if (stop_early && i > 0 && !(fabs(dii) > a.rel_tol * s_r00)) {
+        s_stop = i;
+        s_tau = -1.0;
+      } else {
+        double tau = 0.0;
+        if (ss != 0.0) {
+          tau = (dii - al) / dii;
+          const double scal = 1.0 / (al - dii);
+          for (int r = i + 1; r < w; ++r) vbuf[r] *= scal;
+          y(i, i) = dii;
+          for (int r = i + 1; r < w; ++r) y(r, i) = vbuf[r];
+        }
+        s_tau = tau;
+      }
+    }
+    __syncthreads();
+    const double tau = s_tau;
+    if (tau < 0.0) break;   // rank reached (uniform)
+    // apply the reflector to columns i+1..n-1 (a warp per column) and downdate the norms
+    for (int c = i + 1 + wid; c < n; c += kWWarps) {
+      if (tau != 0.0) {
+        double d = lane == 0 ? y(i, c) : 0.0;
+        for (int r = i + 1 + lane; r < w; r += 32) d += vbuf[r] * y(r, c);
+        d = tau * warp_sum(d);
+        if (lane == 0) y(i, c) -= d;
+        for (int r = i + 1 + lane; r < w; r += 32) y(r, c) -= d * vbuf[r];
+      }
+      __syncwarp();
+      double nv = vn1[c];
+      if (nv != 0.0) {
+        double temp = fabs(y(i, c)) / nv;
+        temp = fmax(1.0 - temp * temp, 0.0);
+        const double q = nv / vn2[c];
+        if (temp * q * q <= tol3z) {
+          double s2 = 0.0;
+          for (int r = i + 1 + lane; r < w; r += 32) s2 += y(r, c) * y(r, c);
+          s2 = warp_sum(s2);
+          if (lane == 0) vn1[c] = vn2[c] = (i + 1 < w) ? sqrt(s2) : 0.0;
+        } else if (lane == 0) {
+          vn1[c] = nv * sqrt(temp);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // rank (id.m:106-113)
+  if (tid == 0) {
+    const int mn_eff = s_stop;
+    const double tol = a.rel_tol * fabs(y(0, 0));
+    int kt = 0;
+    for (int i = 0; i < mn_eff; ++i) kt += fabs(y(i, i)) > tol;
+    int kmax = a.kmax;
+    if (kmax == 0 || kmax > n) kmax = n;
+    s_ktol = kt;
+    s_k = min(kt, kmax);
+    s_niter = 0;
+    s_cap = 0;
+  }
+  __syncthreads();
+  int k = s_k;
+  const int ktol = s_ktol;
+  // clear the reflectors below the diagonal of the first ktol rows (R is upper trapezoidal)
+  for (int c = wid; c < min(ktol, n); c += kWWarps)
+    for (int r = c + 1 + lane; r < ktol; r += 32) y(r, c) = 0.0;
+  __syncthreads();
+  // T = R11 \ R12, a warp per column: right-hand side in registers (row 32 q + lane)
+  if (k > 0 && k < n) {
+    for (int c = k + wid; c < n; c += kWWarps) {
+      double b[kWMaxRows / 32];
+#pragma unroll
+      for (int q = 0; q < kWMaxRows / 32; ++q) {
+        const int r = 32 * q + lane;
+        b[q] = r < k ? y(r, c) : 0.0;
+      }
+      for (int i = k - 1; i >= 0; --i) {
+        const int qi = i >> 5, li = i & 31;
+        double bi = 0.0;
+#pragma unroll
+        for (int q = 0; q < kWMaxRows / 32; ++q)
+          if (q == qi) bi = b[q];
+        const double xi = __shfl_sync(0xffffffffu, bi, li) / y(i, i);
+        const double* Ri = &y(0, i);
+#pragma unroll
+        for (int q = 0; q < kWMaxRows / 32; ++q) {
+          const int r = 32 * q + lane;
+          if (q <= qi) {
+            if (r < i) b[q] -= xi * Ri[r];
+            else if (r == i) b[q] = xi;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kWMaxRows / 32; ++q) {
+        const int r = 32 * q + lane;
+        if (r < k) y(r, c) = b[q];
+      }
+    }
+  }
+  __syncthreads();
+  // RRQR refinement (id.m:117-236), on thread 0, when some |T| > Tmax or rows were cut
+  if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
+    double mx = 0.0;
+    for (int c = k + tid; c < n; c += kWThreads)
+      for (int i = 0; i < k; ++i) mx = fmax(mx, y(i, c) * y(i, c));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    if (lane == 0) red[wid] = mx;
+    __syncthreads();
+    if (tid == 0) {
+      double bm = 0.0;
+      for (int q = 0; q < kWWarps; ++q) bm = fmax(bm, red[q]);
+      s_need = (ktol > k || bm > a.Tmax * a.Tmax) ? 1 : 0;
+      if (s_need) {
+        int niter = 0, capped = 0;
+        const double tol = a.rel_tol * fabs(y(0, 0));
+        s_k = rrqr_serial(Y, 1, w, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped);
+        s_niter = niter;
+        s_cap = capped;
+      }
+    }
+    __syncthreads();
+    k = s_k;
+  }
+  // outputs: [sk rd] order of slf, local permutation, T
+  const int r = n - k;
+  int* perm_out = a.permpool + t.perm_off;
+  int64_t* tmp_ids = reinterpret_cast<int64_t*>(aux);
+  for (int q = tid; q < n; q += kWThreads) tmp_ids[q] = slf[q];
+  __syncthreads();
+  const bool keep_order = r == 0;
+  for (int q = tid; q < n; q += kWThreads) {
+    const int src = keep_order ? q : jpvt[q];
+    perm_out[q] = src;
+    slf[q] = tmp_ids[src];
+  }
+  if (r > 0 && k > 0) {
+    double* T = a.tpool + t.T_off;
+    for (int c = k + wid; c < n; c += kWWarps)
+      for (int i = lane; i < k; i += 32) T[i + (int64_t)(c - k) * k] = y(i, c);
+  }
+  if (tid == 0) {
+    int st = s_cap ? (int)ST_RRQR_CAP : 0;
+    if (k > w - t.ax_guard) st |= ST_ID_CHECK;
+    *out = CompressOut{k, w, s_niter, st};
+  }
+}
+
+}  // namespace
+
+int64_t cpqr_wide_scratch_doubles(int n) { return 8 * (int64_t)n + n / 2 + 2; }
+
+void launch_cpqr_wide(const CompressArgs& a, int ntask, cudaStream_t s) {
+  if (ntask <= 0) return;
+  k_cpqr_wide<<<ntask, kWThreads, 0, s>>>(a);
+}
+
+}  // namespace flam

@@ -550,7 +550,424 @@ __global__ void __launch_bounds__(kThreads) k_eliminate_big(ElimArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- boxes eliminated by many CTAs
+// A box whose redundant block is large (the few boxes near the root in 3D, the root of a
+// 2D tree) is eliminated by a sequence of grid-wide launches instead of one CTA: the same
+// algebra as k_eliminate_big (rskelf.m:219-257), with every O(n^3) part a batched FP64
+// GEMM on the tensor path (mma.sync m8n8k4 .f64) over 64 x 64 tiles, and the LU panels
+// (kHb columns, partial pivoting as xGETF2) factored by one CTA per box.  blockIdx.z is
+// the box within the launch's task list; a box whose r is exhausted leaves at once.
+
+constexpr int kHb = 64;         // LU / solve panel width
+constexpr int kGk = 16;         // GEMM k-chunk
+constexpr int kGld = kGk + 4;   // shared row stride: 20 = 4 mod 16
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+// Views of one box's work matrix (K: n x n, ld n, [sk rd] order) for each GEMM kind.
+enum HbKind { HB_TROW = 0, HB_TCOL, HB_TRAIL, HB_TRAIL_CHOL, HB_EUPD, HB_GUPD, HB_SCHUR };
+
+struct HbOp {
+  double* C;
+  int64_t crs, ccs;
+  GV A, B;
+  int M, N, K;
+};
+
+__device__ __forceinline__ HbOp hb_op(const ElimArgs& a, const ElimTask& t, int kind, int j0) {
+  const int n = t.n, k = t.k, r = n - k;
+  const int64_t ld = n;
+  double* K = a.scratch + t.scr_off;
+  double* Kr = K + k + (int64_t)k * n;
+  const int jb = min(kHb, r - j0), j1 = j0 + jb;
+  const double* T = a.tpool + t.T_off;
+  HbOp o{};
+  switch (kind) {
+    case HB_TROW:   // K(rd,:) -= T' K(sk,:)
+      o = HbOp{K + k, 1, ld, GV{T, k, 1}, GV{K, 1, ld}, r, n, k};
+      break;
+    case HB_TCOL:   // K(:,rd) -= K(:,sk) T
+      o = HbOp{K + (int64_t)k * n, 1, ld, GV{K, 1, ld}, GV{T, 1, k}, n, r, k};
+      break;
+    case HB_TRAIL:  // A22 -= L21 U12
+      o = HbOp{Kr + j1 + (int64_t)j1 * n, 1, ld, GV{Kr + j1 + (int64_t)j0 * n, 1, ld},
+               GV{Kr + j0 + (int64_t)j1 * n, 1, ld}, r - j1, r - j1, jb};
+      break;
+    case HB_TRAIL_CHOL:   // A22 -= L21 L21'
+      o = HbOp{Kr + j1 + (int64_t)j1 * n, 1, ld, GV{Kr + j1 + (int64_t)j0 * n, 1, ld},
+               GV{Kr + j1 + (int64_t)j0 * n, ld, 1}, r - j1, r - j1, jb};
+      break;
+    case HB_EUPD: {   // E(:, j1:) -= E(:, j0:j1) U(j0:j1, j1:)
+      double* E = K + (int64_t)k * n;
+      const GV U12 = a.symm == 'p' ? GV{Kr + j1 + (int64_t)j0 * n, ld, 1} : GV{Kr + j0 + (int64_t)j1 * n, 1, ld};
+      o = HbOp{E + (int64_t)j1 * n, 1, ld, GV{E + (int64_t)j0 * n, 1, ld}, U12, k, r - j1, jb};
+      break;
+    }
+    case HB_GUPD: {   // G(j1:, :) -= L(j1:, j0:j1) G(j0:j1, :)
+      double* G = K + k;
+      o = HbOp{G + j1, 1, ld, GV{Kr + j1 + (int64_t)j0 * n, 1, ld}, GV{G + j0, 1, ld}, r - j1, k, jb};
+      break;
+    }
+    default: {        // HB_SCHUR: M_new -= E G (E E' for 'p')
+      const GV E{K + (int64_t)k * n, 1, ld};
+      const GV Bm = a.symm == 'p' ? GV{K + (int64_t)k * n, ld, 1} : GV{K + k, 1, ld};
+      o = HbOp{a.m_out + t.M_out, 1, k, E, Bm, k, k, r};
+      break;
+    }
+  }
+  return o;
+}
+
+// C tile (64 x 64) -= A B for the box's operation: 4 warps, each 32 x 32 outputs.
+__global__ void __launch_bounds__(128) k_hb_gemm(ElimArgs a, int kind, int j0) {
+  __shared__ double As[kTM * kGld];
+  __shared__ double Bs[kTN * kGld];
+  const ElimTask t = a.tasks[blockIdx.z];
+  const int r = t.n - t.k;
+  if (r <= 0 || j0 >= r) return;
+  if ((kind == HB_TROW || kind == HB_TCOL || kind == HB_EUPD || kind == HB_GUPD || kind == HB_SCHUR) && t.k == 0)
+    return;
+  const HbOp o = hb_op(a, t, kind, j0);
+  const int i0 = blockIdx.x * kTM, c0 = blockIdx.y * kTN;
+  if (i0 >= o.M || c0 >= o.N || o.K <= 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = warp >> 1, wn = warp & 1;
+  const bool a_col = o.A.rs == 1, b_col = o.B.rs == 1;
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  double ra[8], rb[8];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 128 * q;
+      const int m = a_col ? (e & 63) : (e >> 4), kk = a_col ? (e >> 6) : (e & 15);
+      ra[q] = (i0 + m < o.M && k0 + kk < o.K) ? o.A.at(i0 + m, k0 + kk) : 0.0;
+      const int nn = b_col ? (e >> 4) : (e & 63), kb = b_col ? (e & 15) : (e >> 6);
+      rb[q] = (c0 + nn < o.N && k0 + kb < o.K) ? o.B.at(k0 + kb, c0 + nn) : 0.0;
+    }
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 128 * q;
+      const int m = a_col ? (e & 63) : (e >> 4), kk = a_col ? (e >> 6) : (e & 15);
+      As[m * kGld + kk] = ra[q];
+      const int nn = b_col ? (e >> 4) : (e & 63), kb = b_col ? (e & 15) : (e >> 6);
+      Bs[nn * kGld + kb] = rb[q];
+    }
+  };
+  load(0);
+  for (int k0 = 0; k0 < o.K; k0 += kGk) {
+    __syncthreads();
+    stash();
+    __syncthreads();
+    if (k0 + kGk < o.K) load(k0 + kGk);   // next chunk's loads in flight during the products
+    const double* Aw = As + (wm * 32 + g) * kGld + tq;
+    const double* Bw = Bs + (wn * 32 + g) * kGld + tq;
+#pragma unroll
+    for (int kk = 0; kk < kGk; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) af[i] = Aw[i * 8 * kGld + kk];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bf[j] = Bw[j * 8 * kGld + kk];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j], af[i], bf[j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = i0 + wm * 32 + i * 8 + g;
+    if (row >= o.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = c0 + wn * 32 + j * 8 + 2 * tq + e;
+        if (col < o.N) o.C[row * o.crs + col * o.ccs] -= acc[i][j][e];
+      }
+  }
+}
+
+// Child lookup of every position (one CTA per box).
+__global__ void __launch_bounds__(kThreads) k_hb_locate(ElimArgs a) {
+  const ElimTask t = a.tasks[blockIdx.x];
+  if (t.n == 0) return;
+  double* K = a.scratch + t.scr_off;
+  int* pchild = reinterpret_cast<int*>(K + (int64_t)t.n * t.n);
+  locate_children(t, a.permpool + t.perm_off, a.children + t.ch_first, pchild, pchild + t.n);
+}
+
+// K = A(slf,slf) + M in [sk rd] order and M_new = M(sk,sk) (the Schur GEMM subtracts E G
+// from it); a box with r = 0 passes its whole block on.  32 x 32 entries per CTA.
+__global__ void __launch_bounds__(kThreads) k_hb_assemble(ElimArgs a) {
+  const ElimTask t = a.tasks[blockIdx.z];
+  const int n = t.n, k = t.k, r = n - k;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  if (i0 >= n || j0 >= n) return;
+  const Problem& P = a.P;
+  const InstParams ip = P.ip[t.inst];
+  double* K = a.scratch + t.scr_off;
+  const int* pchild = reinterpret_cast<const int*>(K + (int64_t)n * n);
+  const MVal mval{a.m_in, a.children + t.ch_first, pchild, pchild + n};
+  const int64_t* slf = a.ipool + t.slf_off;
+  double* Mo = a.m_out + t.M_out;
+  const int i = i0 + (threadIdx.x & 31);
+  if (i >= n) return;
+  const int64_t si = slf[i];
+  for (int j = j0 + (threadIdx.x >> 5); j < min(n, j0 + 32); j += kThreads / 32) {
+    const double mv = mval(i, j);
+    if (r == 0) {
+      Mo[i + (int64_t)j * n] = mv;
+      continue;
+    }
+    K[i + (int64_t)j * n] = aentry(P, ip, si, slf[j]) + mv;
+    if (i < k && j < k) Mo[i + (int64_t)j * k] = mv;
+  }
+}
+
+// LU (or Cholesky) of the panel rows j0.., columns j0..j1 of K(rd,rd), one CTA per box.
+__global__ void __launch_bounds__(kThreads) k_hb_panel(ElimArgs a, int j0) {
+  __shared__ AM red[kWarps];
+  __shared__ int s_piv;
+  const ElimTask t = a.tasks[blockIdx.x];
+  const int n = t.n, k = t.k, r = n - k;
+  if (r <= 0 || j0 >= r) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double* K = a.scratch + t.scr_off;
+  int* piv = reinterpret_cast<int*>(K + (int64_t)n * n) + 2 * n;
+  double* Kr = K + k + (int64_t)k * n;
+  auto kr = [&](int i, int j) -> double& { return Kr[i + (int64_t)j * n]; };
+  const int jb = min(kHb, r - j0), j1 = j0 + jb;
+  if (a.symm == 'p') {
+    for (int j = j0; j < j1; ++j) {
+      const double dj = kr(j, j);
+      if (!(dj > 0.0)) {
+        if (tid == 0) atomicOr(a.status, (int)ST_NOT_SPD);
+        return;
+      }
+      const double lj = sqrt(dj);
+      __syncthreads();
+      for (int q = j + 1 + tid; q < r; q += kThreads) kr(q, j) /= lj;
+      if (tid == 0) kr(j, j) = lj;
+      __syncthreads();
+      for (int q = j + 1 + tid; q < r; q += kThreads) {
+        const double lq = kr(q, j);
+        for (int c = j + 1; c < min(j1, q + 1); ++c) kr(q, c) -= lq * kr(c, j);
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  for (int j = j0; j < j1; ++j) {
+    AM am{-1.0, r};
+    for (int q = j + tid; q < r; q += kThreads) am = amax(am, AM{fabs(kr(q, j)), q});
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      AM b{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+      am = amax(am, b);
+    }
+    if (lane == 0) red[wid] = am;
+    __syncthreads();
+    if (tid == 0) {
+      AM bm = red[0];
+      for (int w = 1; w < kWarps; ++w) bm = amax(bm, red[w]);
+      const int pv0 = (bm.i >= j && bm.i < r) ? bm.i : j;
+      s_piv = pv0;
+      piv[j] = pv0;
+    }
+    __syncthreads();
+    const int pv = s_piv;
+    if (pv != j && tid < jb) {
+      const double x = kr(j, j0 + tid);
+      kr(j, j0 + tid) = kr(pv, j0 + tid);
+      kr(pv, j0 + tid) = x;
+    }
+    __syncthreads();
+    const double dj = kr(j, j);
+    if (dj == 0.0 && tid == 0) atomicOr(a.status, (int)ST_SINGULAR);
+    // scale column j and update the rest of the panel row by row
+    for (int q = j + 1 + tid; q < r; q += kThreads) {
+      const double lq = dj != 0.0 ? kr(q, j) / dj : kr(q, j);
+      kr(q, j) = lq;
+      for (int c = j + 1; c < j1; ++c) kr(q, c) -= lq * kr(j, c);
+    }
+    __syncthreads();
+  }
+}
+
+// The panel's row interchanges on every column of K(rd,:) outside the panel.
+__global__ void __launch_bounds__(kThreads) k_hb_swap(ElimArgs a, int j0) {
+  const ElimTask t = a.tasks[blockIdx.z];
+  const int n = t.n, k = t.k, r = n - k;
+  if (r <= 0 || j0 >= r) return;
+  const int col = blockIdx.x * kThreads + threadIdx.x;
+  const int j1 = min(j0 + kHb, r);
+  if (col >= n || (col >= k + j0 && col < k + j1)) return;
+  double* K = a.scratch + t.scr_off;
+  const int* piv = reinterpret_cast<const int*>(K + (int64_t)n * n) + 2 * n;
+  double* Kc = K + k + (int64_t)col * n;
+  for (int j = j0; j < j1; ++j) {
+    const int pv = piv[j];
+    if (pv != j) {
+      const double x = Kc[j];
+      Kc[j] = Kc[pv];
+      Kc[pv] = x;
+    }
+  }
+}
+
+// Triangular solves with the panel's diagonal block, one thread per vector:
+// op 0: U12 = L11 \ A12 (columns j1.. of K(rd,rd)); op 1: E(:, j0:j1) /= U11 (rows of
+// K(sk,rd)); op 2: G(j0:j1, :) = L11 \ G(j0:j1, :) (columns of K(rd,sk)).
+__global__ void __launch_bounds__(128) k_hb_trsm(ElimArgs a, int j0, int op) {
+  __shared__ double blk[kHb * (kHb + 1)];
+  const ElimTask t = a.tasks[blockIdx.z];
+  const int n = t.n, k = t.k, r = n - k;
+  if (r <= 0 || j0 >= r || (op > 0 && k == 0)) return;
+  const int jb = min(kHb, r - j0), j1 = j0 + jb;
+  const int nvec = op == 0 ? r - j1 : k;
+  const int v0 = blockIdx.x * 128;
+  if (v0 >= nvec) return;
+  double* K = a.scratch + t.scr_off;
+  double* Kr = K + k + (int64_t)k * n;
+  const bool chol = a.symm == 'p';
+  for (int e = threadIdx.x; e < jb * jb; e += 128) {   // blk(i, c) = U(i, c) or L(i, c) of the diagonal block
+    const int i = e % jb, c = e / jb;
+    blk[i + c * (kHb + 1)] = (op == 1 && chol) ? Kr[(j0 + c) + (int64_t)(j0 + i) * n] : Kr[(j0 + i) + (int64_t)(j0 + c) * n];
+  }
+  __syncthreads();
+  const int v = v0 + threadIdx.x;
+  if (v >= nvec) return;
+  double x[kHb];
+  if (op == 1) {   // row v of E: x U11 = e
+    double* C = K + (int64_t)k * n;
+#pragma unroll
+    for (int c = 0; c < kHb; ++c) {
+      if (c < jb) {
+        double s = C[v + (int64_t)(j0 + c) * n];
+#pragma unroll
+        for (int l = 0; l < c; ++l) s -= x[l] * blk[l + c * (kHb + 1)];
+        x[c] = s / blk[c + c * (kHb + 1)];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kHb; ++c)
+      if (c < jb) C[v + (int64_t)(j0 + c) * n] = x[c];
+    return;
+  }
+  double* col = op == 0 ? Kr + j0 + (int64_t)(j1 + v) * n : K + k + j0 + (int64_t)v * n;
+#pragma unroll
+  for (int i = 0; i < kHb; ++i) {
+    if (i < jb) {
+      double s = col[i];
+#pragma unroll
+      for (int l = 0; l < i; ++l) s -= blk[i + l * (kHb + 1)] * x[l];
+      x[i] = s;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kHb; ++i)
+    if (i < jb) col[i] = x[i];
+}
+
+// Store the factor [T | LU (L) | E | G] and the LU row permutation.
+__global__ void __launch_bounds__(kThreads) k_hb_store(ElimArgs a) {
+  const ElimTask t = a.tasks[blockIdx.z];
+  const int n = t.n, k = t.k, r = n - k;
+  if (r <= 0) return;
+  const bool chol = a.symm == 'p';
+  double* K = a.scratch + t.scr_off;
+  const double* T = a.tpool + t.T_off;
+  double* F = a.fpool + t.fac_off;
+  const int64_t kr_ = (int64_t)k * r, rr = (int64_t)r * r;
+  const int64_t total = 2 * kr_ + rr + (chol ? 0 : kr_);
+  for (int64_t e = blockIdx.x * (int64_t)kThreads + threadIdx.x; e < total; e += (int64_t)gridDim.x * kThreads) {
+    double v;
+    if (e < kr_) {
+      v = T[e];
+    } else if (e < kr_ + rr) {
+      const int64_t q = e - kr_;
+      const int i = (int)(q % r), j = (int)(q / r);
+      v = (chol && i < j) ? 0.0 : K[(k + i) + (int64_t)(k + j) * n];
+    } else if (e < 2 * kr_ + rr) {
+      const int64_t q = e - kr_ - rr;
+      const int i = (int)(q % k), j = (int)(q / k);
+      v = K[i + (int64_t)(k + j) * n];
+    } else {
+      const int64_t q = e - 2 * kr_ - rr;
+      const int i = (int)(q % r), j = (int)(q / r);
+      v = K[(k + i) + (int64_t)j * n];
+    }
+    F[e] = v;
+  }
+  if (!chol && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int* piv = reinterpret_cast<const int*>(K + (int64_t)n * n) + 2 * n;
+    int32_t* pp = a.ppool + t.piv_off;
+    for (int q = 0; q < r; ++q) pp[q] = q;
+    for (int q = 0; q < r; ++q) {
+      const int32_t x = pp[q];
+      pp[q] = pp[piv[q]];
+      pp[piv[q]] = x;
+    }
+  }
+}
+
 }  // namespace
+
+void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int rmax, cudaStream_t s) {
+  if (nbox <= 0 || rmax <= 0) return;
+  const unsigned z = (unsigned)nbox;
+  auto tiles = [](int x) { return (unsigned)std::max(1, (x + 63) / 64); };
+  auto gemm = [&](int kind, int j0, int M, int N) {
+    k_hb_gemm<<<dim3(tiles(M), tiles(N), z), 128, 0, s>>>(a, kind, j0);
+  };
+  k_hb_locate<<<nbox, kThreads, 0, s>>>(a);
+  k_hb_assemble<<<dim3((nmax + 31) / 32, (nmax + 31) / 32, z), kThreads, 0, s>>>(a);
+  if (kmax > 0) {
+    gemm(HB_TROW, 0, rmax, nmax);
+    gemm(HB_TCOL, 0, nmax, rmax);
+  }
+  const bool chol = a.symm == 'p';
+  for (int j0 = 0; j0 < rmax; j0 += kHb) {
+    const int rest = rmax - std::min(rmax, j0 + kHb);
+    k_hb_panel<<<nbox, kThreads, 0, s>>>(a, j0);
+    if (!chol) {
+      k_hb_swap<<<dim3((nmax + kThreads - 1) / kThreads, 1, z), kThreads, 0, s>>>(a, j0);
+      if (rest > 0) k_hb_trsm<<<dim3((rest + 127) / 128, 1, z), 128, 0, s>>>(a, j0, 0);
+    }
+    if (rest > 0) gemm(chol ? HB_TRAIL_CHOL : HB_TRAIL, j0, rest, rest);
+  }
+  if (kmax > 0) {
+    for (int j0 = 0; j0 < rmax; j0 += kHb) {
+      const int rest = rmax - std::min(rmax, j0 + kHb);
+      k_hb_trsm<<<dim3((kmax + 127) / 128, 1, z), 128, 0, s>>>(a, j0, 1);
+      if (rest > 0) gemm(HB_EUPD, j0, kmax, rest);
+      if (!chol) {
+        k_hb_trsm<<<dim3((kmax + 127) / 128, 1, z), 128, 0, s>>>(a, j0, 2);
+        if (rest > 0) gemm(HB_GUPD, j0, rest, kmax);
+      }
+    }
+    gemm(HB_SCHUR, 0, kmax, kmax);
+  }
+  const int64_t tot = 4 * (int64_t)std::max(kmax, 1) * rmax + (int64_t)rmax * rmax;
+  k_hb_store<<<dim3((unsigned)std::min<int64_t>((tot + kThreads - 1) / kThreads, 4096), 1, z), kThreads, 0, s>>>(a);
+}
+
+int elim_huge_launches(int rmax, int kmax, bool chol) {
+  const int np = (rmax + kHb - 1) / kHb;
+  return 3 + (kmax > 0 ? 2 : 0) + np * (chol ? 2 : 4) + (kmax > 0 ? np * (chol ? 2 : 4) + 1 : 0);
+}
 
 size_t elim_smem_bytes(int n) {
   if (n > kSmemN) return sizeof(int) * 3 * (size_t)n + 64;

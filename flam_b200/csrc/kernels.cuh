@@ -41,6 +41,10 @@ int compress_tc_threads(int n);
 int compress_tc_group(int n);
 int compress_tc_rows(int n);
 void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, size_t smem, cudaStream_t s);
+// ID of the explicit row sketch of boxes with n > kTcMaxN (ax_rows <= 1024 rows), one CTA
+// per box; scratch: cpqr_wide_scratch_doubles(n) at the task's scr_off.
+int64_t cpqr_wide_scratch_doubles(int n);
+void launch_cpqr_wide(const CompressArgs& a, int ntask, cudaStream_t s);
 // Neighbour filter alone (row-split form): tasks[0, ntask) compact their candidates
 // and write the kept count to a.mfilt[out_idx].
 void launch_filter(const CompressArgs& a, int ntask, cudaStream_t s);
@@ -67,6 +71,13 @@ int elim_pan_rows_max();
 int64_t elim_scratch_doubles(int n);
 // tasks[0, nsmall): n <= kSmemN (shared-memory kernel); tasks[nsmall, nsmall + nbig): the rest.
 void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cudaStream_t s);
+// Boxes a.tasks[0, nbox) (work matrices in global scratch) eliminated by grid-wide launches:
+// batched FP64 tensor-path GEMMs and one CTA per box for each LU panel.  nmax, kmax, rmax:
+// the largest n, k and r among them.
+void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int rmax, cudaStream_t s);
+int elim_huge_launches(int rmax, int kmax, bool chol);
+// Redundant blocks from this size up take the grid-wide elimination.
+constexpr int kHugeR = 320;
 
 // Segmented copies of int64 ids: dst[dst_off + i] = src[src_off + i], i < len.
 struct CopySeg {

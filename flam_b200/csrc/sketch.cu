@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
   const SketchTask t = a.tasks[blockIdx.x];
   const Problem& P = a.P;
   const InstParams ip = P.ip[t.inst];
-  const int n = t.n, w = t.w, d = P.d;
+  const int n = t.ncol, w = t.nw, d = P.d;        // this CTA's columns of K and rows of Y
   const int MT = (n + 127) / 128;                  // M tiles of 128 columns of K
   const int NP = (w + 15) / 16 * 16;               // N padded
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
   const int cpass = MT * 128;
   const int c = tid % cpass;
   const int rq0 = tid / cpass, rqs = kSkThreads / cpass;
-  const int64_t sc = c < n ? a.ipool[t.slf_off + c] : -1;
+  const int64_t sc = c < n ? a.ipool[t.slf_off + t.col0 + c] : -1;
   double xc[kMaxDim] = {0.0, 0.0, 0.0};
   float nc[2] = {0.f, 0.f};
   double wc = 1.0;
@@ -190,7 +190,11 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
     if (ip.has_w) wc = P.w[sc];
   }
   const int64_t* cand = a.cpool + t.cand_off;
-  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NP >> 3) << 17) | ((128u >> 4) << 24);
+  // instruction descriptor: FP32 accumulate, TF32 A and B, both K-major, M = 128; N = 256 for
+  // the first 256 rows of Y, the rest in a second product
+  const int N0 = NP > 256 ? 256 : NP, N1 = NP - N0;
+  const uint32_t idesc0 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N0 >> 3) << 17) | ((128u >> 4) << 24);
+  const uint32_t idesc1 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N1 >> 3) << 17) | ((128u >> 4) << 24);
   const uint32_t lboA = 16 * 128, lboB = (uint32_t)(NP / 8) * 128;
   uint32_t phase = 0;
   bool issued = false;
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int rho = r0 + rq * 4 + i;
-        o[i] = (j < w && rho < m) ? omega(a.seed, t.box, rho, j) : 0.f;
+        o[i] = (j < w && rho < m) ? omega(a.seed, t.box, rho, t.j0 + j) : 0.f;
       }
       const int off = (rq * (NP / 8) + (j >> 3)) * 32 + (j & 7) * 4;
       *reinterpret_cast<float4*>(Bm + off) = make_float4(o[0], o[1], o[2], o[3]);
@@ -298,10 +302,17 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
         const uint32_t bb = smem_u32(Bm);
         for (int s = 0; s < kKc / 8; ++s) {
           // K slices 2s, 2s+1 (8 rows of K) of every operand
-          const uint64_t bd = smem_desc(bb + (uint32_t)(2 * s) * lboB, lboB, 128);
-          mma_tf32(tmem + (uint32_t)(tm * NP), smem_desc(ahi + (uint32_t)(2 * s) * lboA, lboA, 128), bd, idesc,
-                   (r0 > 0 || s > 0) ? 1u : 0u);
-          mma_tf32(tmem + (uint32_t)(tm * NP), smem_desc(alo + (uint32_t)(2 * s) * lboA, lboA, 128), bd, idesc, 1u);
+          const uint64_t ah = smem_desc(ahi + (uint32_t)(2 * s) * lboA, lboA, 128);
+          const uint64_t al = smem_desc(alo + (uint32_t)(2 * s) * lboA, lboA, 128);
+          const uint32_t acc = (r0 > 0 || s > 0) ? 1u : 0u;
+          const uint64_t bd0 = smem_desc(bb + (uint32_t)(2 * s) * lboB, lboB, 128);
+          mma_tf32(tmem + (uint32_t)(tm * NP), ah, bd0, idesc0, acc);
+          mma_tf32(tmem + (uint32_t)(tm * NP), al, bd0, idesc0, 1u);
+          if (N1 > 0) {   // rows 256.. of the B operand: 32 core matrices further on
+            const uint64_t bd1 = smem_desc(bb + (uint32_t)(2 * s) * lboB + 32 * 128, lboB, 128);
+            mma_tf32(tmem + (uint32_t)(tm * NP + 256), ah, bd1, idesc1, acc);
+            mma_tf32(tmem + (uint32_t)(tm * NP + 256), al, bd1, idesc1, 1u);
+          }
         }
       }
       mma_commit(barp);
@@ -319,7 +330,7 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
     if (tid == 0) atomicOr(a.status, (int)ST_TIMEOUT);
     if (issued && warp == 0 && lane == 0) bar_wait(barp, phase);   // let the products in flight drain (bounded)
   } else if (!issued) {
-    for (int e = tid; e < w * n; e += kSkThreads) Y[e] = 0.0;
+    for (int e = tid; e < w * n; e += kSkThreads) Y[(t.j0 + e % w) + (int64_t)(t.col0 + e / w) * t.w] = 0.0;
   } else {
     // warp: lanes 32 (warp % 4) .. +31 of the accumulator (columns of K), one half of its columns
     const int lq = warp & 3, half = warp >> 2;
@@ -337,7 +348,7 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
         if (cc < n)
 #pragma unroll
           for (int q = 0; q < 8; ++q)
-            if (jb + q < w) Y[(jb + q) + (int64_t)cc * w] = (double)__uint_as_float(r[q]);
+            if (jb + q < w) Y[(t.j0 + jb + q) + (int64_t)(t.col0 + cc) * t.w] = (double)__uint_as_float(r[q]);
       }
     }
   }
@@ -360,8 +371,8 @@ __global__ void k_unpermute(const int32_t* idx, const SketchTask* tasks, int64_t
 
 }  // namespace
 
-size_t sketch_smem_bytes(int n, int w) {
-  const int MT = (n + 127) / 128, NP = (w + 15) / 16 * 16;
+size_t sketch_smem_bytes(int ncol, int nw) {
+  const int MT = (ncol + 127) / 128, NP = (nw + 15) / 16 * 16;
   return 1024 + sizeof(float) * (size_t)(2 * MT * 128 * kKc + NP * kKc);
 }
 

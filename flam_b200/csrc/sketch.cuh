@@ -6,8 +6,12 @@ namespace flam {
 
 // Boxes up to this many points are sketched (two 128-column tiles of tensor memory);
 // larger boxes take the exact compression.
-constexpr int kSketchMaxN = 256;
-constexpr int kSketchMaxW = 256;
+constexpr int kSketchMaxN = 8192;
+constexpr int kSketchMaxW = 1024;
+// One CTA sketches at most this many columns of K and rows of Y (tensor memory: 512 FP32
+// columns of 128 lanes, i.e. tiles x padded rows <= 512).
+constexpr int kSketchCtaCols = 256;
+constexpr int kSketchCtaRows = 512;
 
 // One box of a factorization step in the sketched form.
 struct SketchTask {
@@ -18,6 +22,9 @@ struct SketchTask {
   int32_t n, w;
   int32_t inst, out_idx;
   int32_t box, flags;  // flags bit0: proxy rows (level > 2)
+  // the part of Y this CTA forms: columns [col0, col0 + ncol) of K, rows [j0, j0 + nw) of Y
+  // (ncol <= 256; nw <= 512 when ncol <= 128, else nw <= 256)
+  int32_t col0, ncol, j0, nw;
   double ctr[kMaxDim];
   double l[kMaxDim];
 };
@@ -35,7 +42,7 @@ struct SketchArgs {
   int32_t* status;        // OR of StatusBits (ST_TIMEOUT)
 };
 
-size_t sketch_smem_bytes(int n, int w);
+size_t sketch_smem_bytes(int ncol, int nw);
 void launch_sketch(const SketchArgs& a, int ntask, size_t smem, cudaStream_t s);
 // Boxes idx[0, nidx) of tasks: restore the slf order the compression permuted (perm_off).
 void launch_unpermute(const int32_t* idx, int nidx, const SketchTask* tasks, int64_t* ipool, const int32_t* permpool,

@@ -116,6 +116,7 @@ typedef struct {
   unsigned sketch_seed;  /* seed of Omega */
   const void* predictor; /* flam_predictor* giving each box's rank estimate, or NULL:
                             w = n + sketch_p (never below the rank) */
+  int rank_log;          /* 1: keep every box's features and rank (flam_rank_log) */
 } flam_opts;
 
 typedef struct flam_factor flam_factor;
@@ -272,6 +273,38 @@ FLAM_API flam_status flam_matvec(const flam_factor* F, const double* X, int64_t 
 FLAM_API flam_status flam_rskelf_ir_sv(const flam_factor* F, const double* B, int64_t ldb, double* X, int64_t ldx,
                                        int64_t nrhs, double ir_tol, int max_iter, int* iters, double* relres);
 
+/* Learned rank predictor -- no counterpart in the reference.  A BF16 MLP
+ * 16 -> 128 -> 128 -> 1 (ReLU, sigmoid output) that maps 16 features of a box (point
+ * count, neighbour count, -log10 tol, aspect, depth, point spread and offset moments,
+ * proxy use, dimension, kernel) to its ID rank as a fraction of its point count; with
+ * opts.sketch and opts.predictor the sketch of a box has w = ceil(pred * n) + sketch_p
+ * rows, and the posterior check sends a box whose rank fills its sketch back to the
+ * exact ID (core/id.m, the judge of the prediction).  Training and inference run on the
+ * GPU with the library's own kernels (tensor-core BF16 products, FP32 accumulation,
+ * FP32 master weights, Adam).  Parameters: FP32, layout W1 (128 x 16, row-major) | b1 |
+ * W2 (128 x 128) | b2 | W3 (128) | b3.  The object lives on the device that was current
+ * at creation; its calls run on the legacy default stream. */
+#define FLAM_PREDICTOR_NFEAT 16
+#define FLAM_PREDICTOR_NPARAM 18817
+typedef struct flam_predictor flam_predictor;
+FLAM_API flam_status flam_predictor_create(uint64_t seed, flam_predictor** P);
+FLAM_API void flam_predictor_free(flam_predictor* P);
+FLAM_API flam_status flam_predictor_get(const flam_predictor* P, float* w);
+FLAM_API flam_status flam_predictor_set(flam_predictor* P, const float* w);
+/* Adam on mean (pred - y)^2 over nsamp samples (X: nsamp x 16 row-major, y: nsamp; host
+ * or device memory), `epochs` passes in shuffled minibatches of `batch`; *loss (may be
+ * NULL) gets the last epoch's mean loss. */
+FLAM_API flam_status flam_predictor_train(flam_predictor* P, const float* X, const float* y, int64_t nsamp, int epochs,
+                                          int batch, float lr, uint64_t seed, float* loss);
+FLAM_API flam_status flam_predictor_eval(const flam_predictor* P, const float* X, int64_t nsamp, float* yhat);
+/* One forward and backward pass: *loss = mean (pred - y)^2 and grad (NPARAM floats) its
+ * gradient, for checking the training kernels. */
+FLAM_API flam_status flam_predictor_grad(const flam_predictor* P, const float* X, const float* y, int64_t nsamp,
+                                         float* loss, float* grad);
+/* The features (count x 16) and rank fractions k/n (count) of every compressed box of a
+ * factorization made with opts.rank_log; call with X = y = NULL for *count. */
+FLAM_API flam_status flam_rank_log(const flam_factor* F, int64_t* count, float* X, float* y);
+
 /* Sizes of a handle. */
 typedef struct {
   int64_t N;          /* total points */
@@ -338,6 +371,9 @@ typedef struct {
   double byte_sweep;
   int64_t n_sketch;        /* boxes whose ID came from a row sketch (opts.sketch) */
   int64_t n_sketch_redo;   /* of those, boxes the posterior check sent to the exact ID */
+  int64_t sketch_rows;     /* sum over the sketched boxes of their sketch rows w */
+  int64_t sketch_rows_k;   /* sum over the same boxes of rows(K), the rows the exact ID folds */
+  int64_t id_rows;         /* rows every ID of the factorization folded (w if sketched, else rows(K)) */
 } flam_prof;
 
 FLAM_API flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset);

@@ -70,3 +70,23 @@ def test_sketch_off_is_the_exact_path():
     x, A, pxy = problems.star(3000, seed=4)
     F0 = fb.rskelf(A, x, 64, 1e-8, pxy, dict(symm="n", profile=True))
     assert F0.profile()["n_sketch"] == 0
+
+
+def test_sketched_wide_boxes_and_grid_elimination_reach_fp64_tolerance():
+    """A 3D sphere whose top boxes hold more than 1024 points (the wide pivoted QR of the
+    sketch) and whose root block takes the grid-wide elimination; the FP64 residual is
+    measured by the on-the-fly matvec."""
+    import torch
+    N = 16384
+    x, A, pxy = problems.sphere(N, p=256, seed=7)
+    F = fb.rskelf(A, x, 64, 1e-6, pxy, dict(symm="n", sketch=1, profile=True))
+    assert F.profile()["n_sketch"] > 0
+    nmax = max(len(f["sk"]) + len(f["rd"]) for f in F.factors()["factors"])
+    assert nmax > 1024
+    B = torch.randn(N, 4, dtype=torch.float64, device="cuda").t().contiguous().t()
+    X = torch.empty_like(B)
+    _, it, rel = F.ir_sv_(B, X, 1e-10, 10)
+    R = torch.empty_like(B)
+    F.matvec_(X, R, B)
+    r = (R.norm(dim=0) / B.norm(dim=0)).max().item()
+    assert r <= 1e-10 and rel.max() <= 1e-10 and it >= 1
