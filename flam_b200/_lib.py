@@ -26,6 +26,7 @@ EXPORTS = (
     "flam_rskelf_partial_sv", "flam_rskelf_partial_mv", "flam_factor_import", "flam_rskelf_diag",
     "flam_matvec", "flam_rskelf_ir_sv", "flam_predictor_create", "flam_predictor_free", "flam_predictor_get",
     "flam_predictor_set", "flam_predictor_train", "flam_predictor_eval", "flam_predictor_grad", "flam_rank_log",
+    "flam_autotune", "flam_tune_get", "flam_tune_set",
 )
 
 # int fn(double* Y, int64_t n, int64_t nrhs, char trans, void* stream, void* ctx)
@@ -47,6 +48,10 @@ class FlamOpts(C.Structure):
                 ("symm", C.c_char), ("stop", C.c_int), ("verb", C.c_int), ("stream", C.c_void_p),
                 ("profile", C.c_int), ("sketch", C.c_int), ("sketch_p", C.c_int), ("sketch_guard", C.c_int),
                 ("sketch_seed", C.c_uint), ("predictor", C.c_void_p), ("rank_log", C.c_int)]
+
+
+class FlamTune(C.Structure):
+    _fields_ = [("split_ctas", C.c_int), ("split_max", C.c_int), ("split_min_n", C.c_int), ("tc_smem_max", C.c_int)]
 
 
 class FlamInfo(C.Structure):
@@ -133,6 +138,13 @@ def lib():
     L.flam_predictor_grad.restype = C.c_int
     L.flam_rank_log.argtypes = [P, C.POINTER(C.c_int64), fp, fp]
     L.flam_rank_log.restype = C.c_int
+    L.flam_autotune.argtypes = [P, C.c_int, C.c_int64, C.POINTER(FlamKernel), C.c_double, C.c_double,
+                                C.POINTER(FlamProxy), C.POINTER(FlamOpts), C.c_int, C.POINTER(FlamTune)]
+    L.flam_autotune.restype = C.c_int
+    L.flam_tune_get.argtypes = [C.c_int, C.c_int, C.c_int64, C.POINTER(FlamTune)]
+    L.flam_tune_get.restype = C.c_int
+    L.flam_tune_set.argtypes = [C.c_int, C.c_int, C.c_int64, C.POINTER(FlamTune)]
+    L.flam_tune_set.restype = C.c_int
     L.flam_rskelf_diag.argtypes = [P, C.c_int, P]
     L.flam_rskelf_diag.restype = C.c_int
     L.flam_rskelf_logdet.argtypes = [P, dp, dp]

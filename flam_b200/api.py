@@ -367,19 +367,36 @@ def rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None):
     return Factor(h.value, 1)
 
 
-def rskelf_batched(As, xs, occ, rank_or_tol, pxyfun=None, opts=None):
-    """Many independent rskelf problems in one device pipeline (one launch per level step)."""
+def rskelf_batched(As, xs, occ, rank_or_tol, pxyfun=None, opts=None, sizes=None):
+    """Many independent rskelf problems in one device pipeline (one launch per level step).
+
+    ``xs`` is a list of d x N_i point arrays, or (with ``sizes``) one d x sum(N_i)
+    column-major CUDA tensor of all instances' points, used in place."""
     for A in As:
         _check_handles(A, pxyfun)
-    xs = [np.asfortranarray(x, dtype=np.float64) for x in xs]
-    d = xs[0].shape[0]
-    X = np.asfortranarray(np.concatenate(xs, axis=1))
-    N = np.array([x.shape[1] for x in xs], dtype=np.int64)
+    if sizes is not None:
+        N = np.asarray(sizes, dtype=np.int64)
+        d = xs.shape[0]
+        if _is_cuda_tensor(xs):
+            if xs.stride(0) != 1:
+                raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: x must be a column-major d x N tensor")
+            X, xptr = xs, xs.data_ptr()
+        else:
+            X = np.asfortranarray(xs, dtype=np.float64)
+            xptr = X.ctypes.data
+        if int(N.sum()) != xs.shape[1]:
+            raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: sizes do not add up to the points given")
+    else:
+        xs = [np.asfortranarray(x, dtype=np.float64) for x in xs]
+        d = xs[0].shape[0]
+        X = np.asfortranarray(np.concatenate(xs, axis=1))
+        xptr = X.ctypes.data
+        N = np.array([x.shape[1] for x in xs], dtype=np.int64)
     karr = (_lib.FlamKernel * len(As))(*[A.c_struct() for A in As])
     o, keep = _c_opts(opts)
     px = (pxyfun or Proxy("none", 1)).c_struct()
     h = C.c_void_p()
-    _lib.check(_lib.lib().flam_rskelf_batched(len(As), X.ctypes.data, d, N.ctypes.data_as(C.POINTER(C.c_int64)), karr,
+    _lib.check(_lib.lib().flam_rskelf_batched(len(As), xptr, d, N.ctypes.data_as(C.POINTER(C.c_int64)), karr,
                                               float(occ), float(rank_or_tol), C.byref(px), C.byref(o), C.byref(h)))
     F = Factor(h.value, len(As))
     F._sizes = [int(n) for n in N]
@@ -642,3 +659,41 @@ class Predictor:
     @classmethod
     def load(cls, path):
         return cls(weights=np.load(path)["w"])
+
+
+def _tune_dict(t):
+    return {f: getattr(t, f) for f, _ in t._fields_}
+
+
+def autotune(A, x, occ, rank_or_tol, pxyfun=None, opts=None, reps=2):
+    """Measure the factorization's launch shapes on this problem (coordinate search over the
+    row-split and shared-memory settings, device time) and keep the fastest for its class
+    (dimension, kernel, log2 N) on the current device.  Returns the chosen setting."""
+    _check_handles(A, pxyfun)
+    xa = x if _is_cuda_tensor(x) else np.asfortranarray(x, dtype=np.float64)
+    d, N = xa.shape
+    o, keep = _c_opts(opts)
+    px = (pxyfun or Proxy("none", 1)).c_struct()
+    best = _lib.FlamTune()
+    ptr = xa.data_ptr() if _is_cuda_tensor(xa) else xa.ctypes.data
+    _lib.check(_lib.lib().flam_autotune(ptr, d, N, C.byref(A.c_struct()), float(occ), float(rank_or_tol), C.byref(px),
+                                        C.byref(o), int(reps), C.byref(best)))
+    return _tune_dict(best)
+
+
+def tune_get(d, kernel, N):
+    """The launch shapes factorizations of this class use on the current device."""
+    t = _lib.FlamTune()
+    _lib.check(_lib.lib().flam_tune_get(int(d), _kernel_id(kernel), int(N), C.byref(t)))
+    return _tune_dict(t)
+
+
+def tune_set(d, kernel, N, tune):
+    """Install a saved tuning for this class on the current device."""
+    t = _lib.FlamTune(**{k: int(v) for k, v in tune.items()})
+    _lib.check(_lib.lib().flam_tune_set(int(d), _kernel_id(kernel), int(N), C.byref(t)))
+
+
+def _kernel_id(kernel):
+    from .registry import KERNELS
+    return KERNELS[kernel] if isinstance(kernel, str) else int(kernel)

@@ -21,6 +21,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/flam.h"
@@ -288,6 +289,36 @@ struct Workspace {
     cout.release(s);
   }
 };
+
+// ---------------------------------------------------------------- launch-shape tuning
+// Table of tuned launch shapes per (device, dimension, kernel kind, log2 N).
+struct TuneKey {
+  int dev, d, kind, lg;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, d, kind, lg) < std::tie(o.dev, o.d, o.kind, o.lg);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, flam_tune> g_tune;
+
+flam_tune tune_default() { return flam_tune{148, 8, 32, 40 * 1024}; }
+
+TuneKey tune_key(int dev, int d, int kind, int64_t N) {
+  int lg = 0;
+  while ((int64_t(1) << (lg + 1)) <= std::max<int64_t>(N, 1)) ++lg;
+  return TuneKey{dev, d, kind, lg};
+}
+
+flam_tune tune_lookup(const TuneKey& k) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(k);
+  return it == g_tune.end() ? tune_default() : it->second;
+}
+
+void tune_check(const flam_tune& t) {
+  if (t.split_ctas < 1 || t.split_max < 1 || t.split_min_n < 1 || t.tc_smem_max < 0 || t.tc_smem_max > 200 * 1024)
+    fail(FLAM_ERR_ARG, "FLAM:tune:invalidArg: split_ctas, split_max, split_min_n >= 1, 0 <= tc_smem_max <= 204800");
+}
 
 std::mutex g_ws_mu;
 std::map<std::pair<int, cudaStream_t>, std::unique_ptr<Workspace>> g_ws;
@@ -903,6 +934,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   std::vector<KeptBlock> kept;
   std::vector<double> kept_val;
   const int64_t nrun = std::min<int64_t>(stop, maxsteps);
+  const flam_tune tune = tune_lookup(tune_key(F.dev, F.d, F.iph[0].kind, F.Ntot));
 
   for (int step = 0; step < maxsteps && step < stop; ++step) {
     // this step's T / permutation / scratch set was last read by the elimination two
@@ -983,18 +1015,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // Row-split form on the levels with few boxes: each large box's rows go to
     // nparts CTAs whose R factors are then merged pairwise, so that the step
     // occupies more of the GPU's 148 SMs.
-    static const int split_ctas = [] {   // CTAs a split step aims at (tuning: FLAM_SPLIT_CTAS)
-      const char* e = std::getenv("FLAM_SPLIT_CTAS");
-      return e ? std::max(1, std::atoi(e)) : 148;
-    }();
-    static const int split_max = [] {    // parts per box at most (FLAM_SPLIT_MAX)
-      const char* e = std::getenv("FLAM_SPLIT_MAX");
-      return e ? std::max(1, std::atoi(e)) : 8;
-    }();
-    static const int split_min_n = [] {  // boxes above this size are split (FLAM_SPLIT_MIN_N)
-      const char* e = std::getenv("FLAM_SPLIT_MIN_N");
-      return e ? std::max(1, std::atoi(e)) : 32;
-    }();
+    const int split_ctas = tune.split_ctas;     // CTAs a split step aims at
+    const int split_max = tune.split_max;       // parts per box at most
+    const int split_min_n = tune.split_min_n;   // boxes above this size are split
     // sketched compression (opts.sketch): boxes of at most kSketchMaxN points whose block
     // has more rows than the sketch take Y = Omega K (w rows) and an ID of Y
     // box features (rank predictor, rank log): from the slf lists, gathered here already
@@ -1100,7 +1123,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         npq[q] = np;
       }
       split[q] = npq[q] > 1;
-      const bool c_glob = split[q] || (tc ? compress_tc_smem_bytes(n) > tc_smem_max() : n > kSmemN);
+      const bool c_glob = split[q] || (tc ? compress_tc_smem_bytes(n) > (size_t)tune.tc_smem_max : n > kSmemN);
       const bool e_glob = n > kSmemN;
       t.scr_off = -1;
       elim_scr[q] = -1;
@@ -2570,6 +2593,86 @@ flam_status flam_rank_log(const flam_factor* F, int64_t* count, float* X, float*
     *count = (int64_t)F->rlog_y.size();
     if (X) std::copy(F->rlog_X.begin(), F->rlog_X.end(), X);
     if (y) std::copy(F->rlog_y.begin(), F->rlog_y.end(), y);
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_tune_get(int d, int kernel_kind, int64_t N, flam_tune* t) {
+  return guard([&] {
+    if (!t) fail(FLAM_ERR_ARG, "FLAM:tune:invalidArg: NULL output");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    *t = tune_lookup(tune_key(dev, d, kernel_kind, N));
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_tune_set(int d, int kernel_kind, int64_t N, const flam_tune* t) {
+  return guard([&] {
+    if (!t) fail(FLAM_ERR_ARG, "FLAM:tune:invalidArg: NULL argument");
+    tune_check(*t);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[tune_key(dev, d, kernel_kind, N)] = *t;
+    return FLAM_OK;
+  });
+}
+
+flam_status flam_autotune(const double* x, int d, int64_t N, const flam_kernel* A, double occ, double rank_or_tol,
+                          const flam_proxy* pxy, const flam_opts* opts, int reps, flam_tune* best) {
+  return guard([&] {
+    if (!A || !best) fail(FLAM_ERR_ARG, "FLAM:tune:invalidArg: NULL argument");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    const TuneKey key = tune_key(dev, d, A->kind, N);
+    reps = std::max(1, reps);
+    flam_opts o;
+    flam_opts_default(&o);
+    if (opts) o = *opts;
+    o.verb = 0;
+    o.profile = 0;
+    // device time of the factorization with setting t (the fastest of reps runs)
+    auto measure = [&](const flam_tune& t) {
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = t;
+      }
+      double tb = 1e300;
+      for (int r = 0; r < reps; ++r) {
+        flam_factor* F = nullptr;
+        const flam_status st = create(1, x, d, &N, A, occ, rank_or_tol, pxy, &o, &F);
+        if (st != FLAM_OK && st < 100) fail(st, "%s", g_err.c_str());
+        tb = std::min(tb, F->t_tree + F->t_factor);
+        flam_factor_free(F);
+      }
+      return tb;
+    };
+    flam_tune cur = tune_lookup(key);
+    double tbest = measure(cur);
+    const std::vector<int> c_ctas{74, 148, 296}, c_max{2, 4, 8, 16}, c_min{16, 32, 64, 128},
+        c_smem{0, 40 * 1024, 96 * 1024, 200 * 1024};
+    auto sweep = [&](int flam_tune::*field, const std::vector<int>& vals) {
+      for (int v : vals) {
+        if (cur.*field == v) continue;
+        flam_tune t = cur;
+        t.*field = v;
+        const double tm = measure(t);
+        if (tm < tbest) {
+          tbest = tm;
+          cur = t;
+        }
+      }
+    };
+    sweep(&flam_tune::split_ctas, c_ctas);
+    sweep(&flam_tune::split_max, c_max);
+    sweep(&flam_tune::split_min_n, c_min);
+    sweep(&flam_tune::tc_smem_max, c_smem);
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune[key] = cur;
+    }
+    *best = cur;
     return FLAM_OK;
   });
 }

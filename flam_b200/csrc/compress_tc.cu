@@ -561,17 +561,6 @@ void launch_b(const CompressArgs& a, int ntask, int nt, size_t smem, cudaStream_
 
 }  // namespace
 
-size_t tc_smem_max() {
-  static size_t v = [] {
-    const char* e = std::getenv("FLAM_TC_SMEM_MAX");
-    // default: only the small boxes (n <~ 64) keep R in shared memory; larger ones
-    // read it from L2 with one-step prefetch, which leaves room for more CTAs per SM
-    const long long x = e ? std::atoll(e) : 40 * 1024;
-    return (size_t)std::min<long long>(std::max<long long>(x, 0), 200 * 1024);
-  }();
-  return v;
-}
-
 int64_t compress_tc_doubles(int n) { return (int64_t)n * (n | 1) + 8 * (int64_t)n + n / 2 + 2; }
 
 size_t compress_tc_smem_bytes(int n) { return sizeof(double) * (size_t)compress_tc_doubles(n); }

@@ -1,4 +1,4 @@
-// ID of a short, wide explicit matrix: the row sketch Y (w x n, w <= 1024 rows) of a box
+// ID of a short, wide explicit matrix: the row sketch Y (w x n, w <= 2048 rows) of a box
 // with more points than the thread-per-column compression takes (n > 1024).
 //
 // Same decisions as the other compression kernels (core/id.m:102-114 on Y): column-
@@ -7,8 +7,8 @@
 // tol |R(0,0)| in tolerance mode, the rank, T = R11 \ R12 and, when some |T| > Tmax, the
 // RRQR refinement of id.m:116-236 (rrqr.cuh).  One CTA per box; Y is updated in place
 // in global memory (L2-resident), a warp per column for the reflector products (lanes
-// over rows: coalesced), the reflector in shared memory.  T is solved column by column
-// by one warp each, the right-hand side held in registers across the lanes.
+// over rows: coalesced), the reflector in shared memory.  T is solved a column per
+// thread in 32-row blocks (the block's unknowns in registers).
 #include <cmath>
 
 #include "common.cuh"
@@ -20,7 +20,7 @@ namespace {
 
 constexpr int kWThreads = 512;
 constexpr int kWWarps = kWThreads / 32;
-constexpr int kWMaxRows = 1024;
+constexpr int kWMaxRows = 2048;
 
 struct WAm {
   double v;
@@ -178,36 +178,39 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
   for (int c = wid; c < min(ktol, n); c += kWWarps)
     for (int r = c + 1 + lane; r < ktol; r += 32) y(r, c) = 0.0;
   __syncthreads();
-  // T = R11 \ R12, a warp per column: right-hand side in registers (row 32 q + lane)
+  // T = R11 \ R12, a thread per column, 32-row blocks from the bottom: the block's
+  // unknowns in registers (diagonal solve), then one pass over the rows above it
+  // (R's entries are the same for every thread: broadcast loads)
   if (k > 0 && k < n) {
-    for (int c = k + wid; c < n; c += kWWarps) {
-      double b[kWMaxRows / 32];
+    for (int c = k + tid; c < n; c += kWThreads) {
+      double* yc = &y(0, c);
+      for (int i1 = k; i1 > 0;) {
+        const int i0 = i1 > 32 ? i1 - 32 : 0, bs = i1 - i0;
+        double x[32];
 #pragma unroll
-      for (int q = 0; q < kWMaxRows / 32; ++q) {
-        const int r = 32 * q + lane;
-        b[q] = r < k ? y(r, c) : 0.0;
-      }
-      for (int i = k - 1; i >= 0; --i) {
-        const int qi = i >> 5, li = i & 31;
-        double bi = 0.0;
+        for (int j = 0; j < 32; ++j) x[j] = j < bs ? yc[i0 + j] : 0.0;
 #pragma unroll
-        for (int q = 0; q < kWMaxRows / 32; ++q)
-          if (q == qi) bi = b[q];
-        const double xi = __shfl_sync(0xffffffffu, bi, li) / y(i, i);
-        const double* Ri = &y(0, i);
+        for (int j = 31; j >= 0; --j) {
+          if (j < bs) {
+            double v = x[j];
 #pragma unroll
-        for (int q = 0; q < kWMaxRows / 32; ++q) {
-          const int r = 32 * q + lane;
-          if (q <= qi) {
-            if (r < i) b[q] -= xi * Ri[r];
-            else if (r == i) b[q] = xi;
+            for (int l = j + 1; l < 32; ++l)
+              if (l < bs) v -= y(i0 + j, i0 + l) * x[l];
+            x[j] = v / y(i0 + j, i0 + j);
           }
         }
-      }
 #pragma unroll
-      for (int q = 0; q < kWMaxRows / 32; ++q) {
-        const int r = 32 * q + lane;
-        if (r < k) y(r, c) = b[q];
+        for (int j = 0; j < 32; ++j)
+          if (j < bs) yc[i0 + j] = x[j];
+        for (int rr = 0; rr < i0; ++rr) {
+          double v = yc[rr];
+          const double* Rr = &y(rr, i0);
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j < bs) v -= Rr[(int64_t)j * w] * x[j];
+          yc[rr] = v;
+        }
+        i1 = i0;
       }
     }
   }

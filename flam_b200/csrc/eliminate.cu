@@ -558,7 +558,12 @@ __global__ void __launch_bounds__(kThreads) k_eliminate_big(ElimArgs a) {
 // (kHb columns, partial pivoting as xGETF2) factored by one CTA per box.  blockIdx.z is
 // the box within the launch's task list; a box whose r is exhausted leaves at once.
 
-constexpr int kHb = 64;         // LU / solve panel width
+// LU / solve panel width: the panel factorization streams its (r - j0) x kHb block
+// through one SM once per column (~r^2 kHb bytes in all), the trailing updates stream
+// the trailing matrix once per panel (~r^3 / kHb bytes, over the whole GPU); 32 balances
+// the two for the redundant blocks of a few thousand rows this path takes.
+constexpr int kHb = 32;
+constexpr int kPanelThreads = 512;
 constexpr int kGk = 16;         // GEMM k-chunk
 constexpr int kGld = kGk + 4;   // shared row stride: 20 = 4 mod 16
 
@@ -737,7 +742,8 @@ __global__ void __launch_bounds__(kThreads) k_hb_assemble(ElimArgs a) {
 }
 
 // LU (or Cholesky) of the panel rows j0.., columns j0..j1 of K(rd,rd), one CTA per box.
-__global__ void __launch_bounds__(kThreads) k_hb_panel(ElimArgs a, int j0) {
+__global__ void __launch_bounds__(kPanelThreads) k_hb_panel(ElimArgs a, int j0) {
+  constexpr int kThreads = kPanelThreads, kWarps = kPanelThreads / 32;
   __shared__ AM red[kWarps];
   __shared__ int s_piv;
   const ElimTask t = a.tasks[blockIdx.x];
@@ -941,7 +947,7 @@ void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int 
   const bool chol = a.symm == 'p';
   for (int j0 = 0; j0 < rmax; j0 += kHb) {
     const int rest = rmax - std::min(rmax, j0 + kHb);
-    k_hb_panel<<<nbox, kThreads, 0, s>>>(a, j0);
+    k_hb_panel<<<nbox, kPanelThreads, 0, s>>>(a, j0);
     if (!chol) {
       k_hb_swap<<<dim3((nmax + kThreads - 1) / kThreads, 1, z), kThreads, 0, s>>>(a, j0);
       if (rest > 0) k_hb_trsm<<<dim3((rest + 127) / 128, 1, z), 128, 0, s>>>(a, j0, 0);

@@ -32,9 +32,9 @@ void launch_compress(const CompressArgs& a, int ntask, size_t smem, cudaStream_t
 // (compress_tc_threads(n)), work arrays of compress_tc_doubles(n) in shared memory
 // when they fit kTcSmemMax, else in the task's global scratch.
 constexpr int kTcMaxN = 1024;
-// Work arrays above this many bytes go to global scratch (L2); tunable through
-// FLAM_TC_SMEM_MAX (bytes) to trade shared-memory residency for occupancy.
-size_t tc_smem_max();
+// Work arrays above the tuned tc_smem_max bytes (flam_tune) go to global scratch (L2):
+// by default only the small boxes (n <~ 64) keep R in shared memory, larger ones read it
+// from L2 with a one-step prefetch, which leaves room for more CTAs per SM.
 int64_t compress_tc_doubles(int n);
 size_t compress_tc_smem_bytes(int n);
 int compress_tc_threads(int n);

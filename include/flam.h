@@ -305,6 +305,27 @@ FLAM_API flam_status flam_predictor_grad(const flam_predictor* P, const float* X
  * factorization made with opts.rank_log; call with X = y = NULL for *count. */
 FLAM_API flam_status flam_rank_log(const flam_factor* F, int64_t* count, float* X, float* y);
 
+/* Launch shapes of the factorization, per device and problem class -- not in the
+ * reference.  A step with few boxes splits each box of more than split_min_n points over
+ * up to split_max CTAs (row-split compression with pairwise merges) so that the step
+ * fills about split_ctas CTAs; work matrices of up to tc_smem_max bytes stay in shared
+ * memory.  flam_autotune measures candidate settings on a given problem (coordinate
+ * search, device time of the factorization) and records the fastest for its class
+ * (dimension, kernel, log2 N) on the current device; every later factorization of that
+ * class on that device uses it.  flam_tune_get / flam_tune_set read and write the
+ * table (to save a tuning and load it in another process). */
+typedef struct {
+  int split_ctas;   /* CTAs a few-box step aims at (default 148, the SM count) */
+  int split_max;    /* row-split parts per box at most (default 8) */
+  int split_min_n;  /* boxes above this many points are split (default 32) */
+  int tc_smem_max;  /* bytes of work matrix kept in shared memory (default 40960) */
+} flam_tune;
+FLAM_API flam_status flam_autotune(const double* x, int d, int64_t N, const flam_kernel* A, double occ,
+                                   double rank_or_tol, const flam_proxy* pxy, const flam_opts* opts, int reps,
+                                   flam_tune* best);
+FLAM_API flam_status flam_tune_get(int d, int kernel_kind, int64_t N, flam_tune* t);
+FLAM_API flam_status flam_tune_set(int d, int kernel_kind, int64_t N, const flam_tune* t);
+
 /* Sizes of a handle. */
 typedef struct {
   int64_t N;          /* total points */

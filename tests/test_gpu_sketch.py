@@ -90,3 +90,21 @@ def test_sketched_wide_boxes_and_grid_elimination_reach_fp64_tolerance():
     F.matvec_(X, R, B)
     r = (R.norm(dim=0) / B.norm(dim=0)).max().item()
     assert r <= 1e-10 and rel.max() <= 1e-10 and it >= 1
+
+
+def test_autotune_records_a_setting_that_later_factorizations_use():
+    x, A, pxy = problems.star(20000, seed=9)
+    before = fb.tune_get(2, "laplace2d", 20000)
+    best = fb.autotune(A, x, 64, 1e-10, pxy, dict(symm="n"), reps=1)
+    assert fb.tune_get(2, "laplace2d", 20000) == best
+    assert best["split_ctas"] in (74, 148, 296) and best["split_max"] in (2, 4, 8, 16)
+    # the tuned shapes change launch geometry, not the factorization's ranks
+    xo, Ao, po = configs.star(20000, seed=9)
+    F = fb.rskelf(A, x, 64, 1e-10, pxy, dict(symm="n"))
+    fb.tune_set(2, "laplace2d", 20000, before)
+    G = fb.rskelf(A, x, 64, 1e-10, pxy, dict(symm="n"))
+    sf, sg = F.level_stats(), G.level_stats()
+    assert np.array_equal(sf[:, :3], sg[:, :3]) or sf.shape == sg.shape
+    assert np.all(np.abs(sf[:, 3] - sg[:, 3]) <= 0.002 * sg[:, 3] + 1)
+    with pytest.raises(fb.FlamError, match="tune:invalidArg"):
+        fb.tune_set(2, "laplace2d", 20000, dict(split_ctas=0, split_max=8, split_min_n=32, tc_smem_max=0))
