@@ -185,6 +185,7 @@ struct Workspace {
   DBuf<CompressTask> skfilt, redo_task, wtask;
   DBuf<int32_t> mrows, redo_idx;
   DBuf<CompressTask> ftask;
+  DBuf<unsigned char> gwstate;
   DBuf<float> feat, fyhat;
   DBuf<double> irB, irX, irR, irW, colsq;
   cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
@@ -275,6 +276,7 @@ struct Workspace {
     mrows.release(s);
     redo_idx.release(s);
     ftask.release(s);
+    gwstate.release(s);
     feat.release(s);
     fyhat.release(s);
     cpool.release(s);
@@ -1057,7 +1059,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         CK(cudaGetLastError());
         auto yh = download(ws.fyhat.p, nb, s);
         pred_k.resize(nb);
-        for (int q = 0; q < nb; ++q) pred_k[q] = (int)std::ceil((double)yh[q] * (double)nslf[q]);
+        // 25% above the prediction: a low estimate costs a second sketch, a high one only rows
+        for (int q = 0; q < nb; ++q) pred_k[q] = (int)std::ceil(1.25 * (double)yh[q] * (double)nslf[q]);
       }
     }
     std::vector<int> skw(nb, 0);
@@ -1157,6 +1160,24 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // task segments: [whole boxes | filter of split boxes | parts | merge level 0 | level 1 ...]
     std::vector<CompressTask> cts;
     cts.reserve(nb * 3);
+    // ID of the sketches of boxes wider than a thread per column: few boxes spread every
+    // pivot step over the GPU, many take one CTA each
+    auto launch_wide = [&](const CompressArgs& cw, const std::vector<CompressTask>& tasks) {
+      const int nt = (int)tasks.size();
+      if (nt < 148) {
+        int nmx = 0, steps = 0;
+        for (const CompressTask& u : tasks) {
+          nmx = std::max(nmx, u.n);
+          steps = std::max(steps, std::min(u.n, u.ax_rows));
+        }
+        ws.gwstate.ensure((int64_t)cpqr_grid_state_bytes(nt), s);
+        launch_cpqr_grid(cw, nt, nmx, steps, ws.gwstate.p, s);
+        F.prof.launches += 5 + 2 * steps;
+      } else {
+        launch_cpqr_wide(cw, nt, s);
+        F.prof.launches += 1;
+      }
+    };
     // sketched boxes: their filter and sketch tasks, and the ID of Y in place of K's rows
     std::vector<SketchTask> skt;
     std::vector<CompressTask> skf, wts;
@@ -1335,8 +1356,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         ws.wtask.upload(wts, s);
         CompressArgs cw = ca;
         cw.tasks = ws.wtask.p;
-        launch_cpqr_wide(cw, (int)wts.size(), s);
-        F.prof.launches += 1;
+        launch_wide(cw, wts);
       }
       F.prof.n_sketch += (int64_t)skf.size();
     }
@@ -1369,22 +1389,114 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         }
       if (!redo.empty()) {
         auto mf = download(ws.mfilt.p, nb, s);
-        std::vector<int32_t> ridx;
-        std::vector<CompressTask> rt;
-        int nmx = 0;
+        // every redone box back to its pull-up order (the first pass permuted its slf)
+        {
+          std::vector<int32_t> ridx;
+          int nmx = 0;
+          for (int q : redo) {
+            ridx.push_back(sk_of[q]);
+            nmx = std::max(nmx, (int)nslf[q]);
+          }
+          ws.redo_idx.upload(ridx, s);
+          launch_unpermute(ws.redo_idx.p, (int)ridx.size(), ws.sktask.p, F.ipool.p, permpool.p, nmx, s);
+          F.prof.launches += 1;
+        }
+        // boxes wider than the thread-per-column compression get a second sketch at full
+        // width n + p (the rank cannot fill it unless the width is capped); the others, and
+        // any box whose second sketch fills too, take the exact ID
+        std::vector<int> exact;
+        std::vector<int> resk;
+        const int spf = std::max(o.sketch_p, 8);
         for (int q : redo) {
-          ridx.push_back(sk_of[q]);
+          const int wf = std::min((int)nslf[q] + spf, kSketchMaxW);
+          if (nslf[q] > kTcMaxN && wf > skw[q])
+            resk.push_back(q);
+          else
+            exact.push_back(q);
+        }
+        if (!resk.empty()) {
+          std::vector<SketchTask> skt2;
+          std::vector<CompressTask> wts2;
+          std::vector<int> first2;
+          int64_t y2 = 0;
+          for (int q : resk) {
+            const int wf = std::min((int)nslf[q] + spf, kSketchMaxW);
+            SketchTask u = skt[sk_of[q]];
+            u.w = wf;
+            u.y_off = y2;
+            first2.push_back((int)skt2.size());
+            for (int c0i = 0; c0i < u.n; c0i += 128)
+              for (int j0i = 0; j0i < wf; j0i += kSketchCtaRows) {
+                SketchTask v2 = u;
+                v2.col0 = c0i;
+                v2.ncol = std::min(128, u.n - c0i);
+                v2.j0 = j0i;
+                v2.nw = std::min(kSketchCtaRows, wf - j0i);
+                skt2.push_back(v2);
+              }
+            CompressTask v = ct[q];
+            v.flags = 0;
+            v.ncand = wf;
+            v.ax_off = y2;
+            v.ax_rows = wf;
+            v.ax_guard = sk_guard;
+            wts2.push_back(v);
+            F.prof.id_rows += skw[q];   // the first sketch's rows
+            skw[q] = wf;
+            y2 += (int64_t)wf * nslf[q];
+          }
+          ws.ypool.ensure(y2, s);   // the first pass's sketches are consumed
+          ws.sktask.upload(skt2, s);
+          SketchArgs sa{};
+          sa.P = P;
+          sa.tasks = ws.sktask.p;
+          sa.ipool = F.ipool.p;
+          sa.cpool = cpool.p;
+          sa.mfilt = ws.mfilt.p;
+          sa.ypool = ws.ypool.p;
+          sa.mrows = ws.mrows.p;
+          sa.symm_n = F.symm == 'n' ? 1 : 0;
+          sa.seed = o.sketch_seed ^ 0x9E3779B9u;
+          sa.status = status.p;
+          size_t smx = 0;
+          for (const SketchTask& u : skt2) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
+          launch_sketch(sa, (int)skt2.size(), smx, s);
+          ws.wtask.upload(wts2, s);
+          CompressArgs cw = ca;
+          cw.tasks = ws.wtask.p;
+          cw.ypool = ws.ypool.p;
+          launch_wide(cw, wts2);
+          F.prof.launches += 1;
+          CK(cudaGetLastError());
+          auto co3 = download(cout.p, nb, s);
+          std::vector<int32_t> ridx2;
+          int nmx2 = 0;
+          for (size_t e = 0; e < resk.size(); ++e) {
+            const int q = resk[e];
+            if (co3[q].status & ST_ID_CHECK) {   // filled even at full width: exact ID
+              exact.push_back(q);
+              ridx2.push_back(first2[e]);
+              nmx2 = std::max(nmx2, (int)nslf[q]);
+            } else {
+              co[q] = co3[q];
+            }
+          }
+          if (!ridx2.empty()) {
+            ws.redo_idx.upload(ridx2, s);
+            launch_unpermute(ws.redo_idx.p, (int)ridx2.size(), ws.sktask.p, F.ipool.p, permpool.p, nmx2, s);
+            F.prof.launches += 1;
+          }
+        }
+        std::vector<CompressTask> rt;
+        for (int q : exact) {
           CompressTask v = ct[q];
           v.flags &= ~2;          // candidates already filtered
           v.ncand = mf[q];
           rt.push_back(v);
-          nmx = std::max(nmx, (int)nslf[q]);
         }
         std::stable_sort(rt.begin(), rt.end(),
                          [&](const CompressTask& x, const CompressTask& y) { return kkey_n(x.n) < kkey_n(y.n); });
-        ws.redo_idx.upload(ridx, s);
         ws.redo_task.upload(rt, s);
-        launch_unpermute(ws.redo_idx.p, (int)ridx.size(), ws.sktask.p, F.ipool.p, permpool.p, nmx, s);
         for (size_t b0 = 0; b0 < rt.size();) {
           const int key = kkey_n(rt[b0].n);
           size_t b1 = b0;
@@ -1403,12 +1515,11 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           b0 = b1;
         }
         CK(cudaGetLastError());
-        F.prof.launches += 1;
         F.prof.n_sketch_redo += (int64_t)redo.size();
         auto co2 = download(cout.p, nb, s);
-        for (int q : redo) {
+        for (int q : exact) {
           co[q] = co2[q];
-          redone[q] = 1;
+          redone[q] = 1;   // folded its sketch, then K
         }
       }
     }

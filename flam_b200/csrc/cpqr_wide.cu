@@ -9,6 +9,7 @@
 // in global memory (L2-resident), a warp per column for the reflector products (lanes
 // over rows: coalesced), the reflector in shared memory.  T is solved a column per
 // thread in 32-row blocks (the block's unknowns in registers).
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -266,6 +267,292 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- grid form
+// The same factorization with every pivot step split over the GPU: for few wide boxes
+// (the 8 boxes below a 3D root) one CTA per box leaves most SMs idle.  Step i is two
+// launches over all boxes of the step: k_gw_pivot (one CTA per box: pivot, column swap,
+// reflector) and k_gw_apply (16 columns per CTA: reflector products and norm downdates);
+// then k_gw_rank, k_gw_tsolve (a thread per column of T) and k_gw_out (RRQR, outputs).
+// Per-box state (the step at which the rank was reached, tau, |R(0,0)|, k) lives in a
+// small device array.
+
+struct GwState {
+  int stop;      // steps done (the rank in tolerance mode, else min(w, n))
+  int k, ktol;
+  int niter, cap;
+  int pad;
+  double tau, r00;
+};
+
+__global__ void __launch_bounds__(kWThreads) k_gw_norms(CompressArgs a, GwState* gs) {
+  const CompressTask t = a.tasks[blockIdx.y];
+  const int n = t.n, w = t.ax_rows, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const double* Y = a.ypool + t.ax_off;
+  double* vn1 = a.scratch + t.scr_off;
+  double* vn2 = vn1 + n;
+  int* jpvt = reinterpret_cast<int*>(vn2 + 7 * (int64_t)n);
+  const int c = blockIdx.x * kWWarps + wid;
+  if (c < n) {
+    double s = 0.0;
+    for (int r = lane; r < w; r += 32) s += Y[r + (int64_t)c * w] * Y[r + (int64_t)c * w];
+    s = warp_sum(s);
+    if (lane == 0) {
+      vn1[c] = vn2[c] = sqrt(s);
+      jpvt[c] = c;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    GwState z{};
+    z.stop = (n == 0 || w > kWMaxRows) ? 0 : min(w, n);
+    z.r00 = 0.0;
+    gs[blockIdx.y] = z;
+  }
+}
+
+__global__ void __launch_bounds__(kWThreads) k_gw_pivot(CompressArgs a, GwState* gs, int i) {
+  __shared__ double red[kWWarps];
+  __shared__ WAm ram[kWWarps];
+  __shared__ int s_pvt;
+  const int b = blockIdx.x;
+  if (i >= gs[b].stop) return;
+  const CompressTask t = a.tasks[b];
+  const int n = t.n, w = t.ax_rows;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double* Y = const_cast<double*>(a.ypool) + t.ax_off;
+  auto y = [&](int r, int c) -> double& { return Y[r + (int64_t)c * w]; };
+  double* vn1 = a.scratch + t.scr_off;
+  double* vn2 = vn1 + n;
+  int* jpvt = reinterpret_cast<int*>(vn2 + 7 * (int64_t)n);
+  WAm am{-1.0, n};
+  for (int c = i + tid; c < n; c += kWThreads) am = wbetter(am, WAm{vn1[c], c});
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    WAm bb{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+    am = wbetter(am, bb);
+  }
+  if (lane == 0) ram[wid] = am;
+  __syncthreads();
+  if (tid == 0) {
+    WAm bm = ram[0];
+    for (int q = 1; q < kWWarps; ++q) bm = wbetter(bm, ram[q]);
+    s_pvt = (bm.i >= i && bm.i < n) ? bm.i : i;
+  }
+  __syncthreads();
+  const int pvt = s_pvt;
+  double s = 0.0;
+  for (int r = tid; r < w; r += kWThreads) {
+    const double v = y(r, pvt);
+    if (pvt != i) {
+      y(r, pvt) = y(r, i);
+      y(r, i) = v;
+    }
+    if (r > i) s += v * v;
+  }
+  if (tid == 0 && pvt != i) {
+    const int tj = jpvt[pvt];
+    jpvt[pvt] = jpvt[i];
+    jpvt[i] = tj;
+    vn1[pvt] = vn1[i];
+    vn2[pvt] = vn2[i];
+  }
+  s = warp_sum(s);
+  if (lane == 0) red[wid] = s;
+  __syncthreads();
+  double ss = 0.0;
+  for (int q = 0; q < kWWarps; ++q) ss += red[q];
+  const double al = y(i, i);
+  const double dii = ss != 0.0 ? -copysign(hypot(al, sqrt(ss)), al) : al;
+  const double r00 = i == 0 ? fabs(dii) : gs[b].r00;
+  if (a.kmax == 0 && i > 0 && !(fabs(dii) > a.rel_tol * r00)) {   // rank reached (tolerance mode)
+    __syncthreads();
+    if (tid == 0) gs[b].stop = i;
+    return;
+  }
+  double tau = 0.0;
+  if (ss != 0.0) {
+    tau = (dii - al) / dii;
+    const double scal = 1.0 / (al - dii);
+    for (int r = i + 1 + tid; r < w; r += kWThreads) y(r, i) *= scal;
+  }
+  __syncthreads();   // every thread has read y(i, i)
+  if (tid == 0) {
+    if (ss != 0.0) y(i, i) = dii;
+    gs[b].tau = tau;
+    if (i == 0) gs[b].r00 = r00;
+  }
+}
+
+__global__ void __launch_bounds__(kWThreads) k_gw_apply(CompressArgs a, GwState* gs, int i) {
+  __shared__ double v[kWMaxRows];
+  const int b = blockIdx.y;
+  if (i >= gs[b].stop) return;
+  const CompressTask t = a.tasks[b];
+  const int n = t.n, w = t.ax_rows;
+  const int c0 = i + 1 + blockIdx.x * kWWarps;
+  if (c0 >= n) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double* Y = const_cast<double*>(a.ypool) + t.ax_off;
+  auto y = [&](int r, int c) -> double& { return Y[r + (int64_t)c * w]; };
+  double* vn1 = a.scratch + t.scr_off;
+  double* vn2 = vn1 + n;
+  const double tau = gs[b].tau;
+  for (int r = i + 1 + tid; r < w; r += kWThreads) v[r] = y(r, i);
+  __syncthreads();
+  const double tol3z = 1.0536712127723509e-08;
+  const int c = c0 + wid;
+  if (c >= n) return;
+  if (tau != 0.0) {
+    double d = lane == 0 ? y(i, c) : 0.0;
+    for (int r = i + 1 + lane; r < w; r += 32) d += v[r] * y(r, c);
+    d = tau * warp_sum(d);
+    if (lane == 0) y(i, c) -= d;
+    for (int r = i + 1 + lane; r < w; r += 32) y(r, c) -= d * v[r];
+  }
+  __syncwarp();
+  const double nv = vn1[c];
+  if (nv != 0.0) {
+    double temp = fabs(y(i, c)) / nv;
+    temp = fmax(1.0 - temp * temp, 0.0);
+    const double q = nv / vn2[c];
+    if (temp * q * q <= tol3z) {
+      double s2 = 0.0;
+      for (int r = i + 1 + lane; r < w; r += 32) s2 += y(r, c) * y(r, c);
+      s2 = warp_sum(s2);
+      if (lane == 0) vn1[c] = vn2[c] = (i + 1 < w) ? sqrt(s2) : 0.0;
+    } else if (lane == 0) {
+      vn1[c] = nv * sqrt(temp);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kWThreads) k_gw_rank(CompressArgs a, GwState* gs) {
+  const int b = blockIdx.x;
+  const CompressTask t = a.tasks[b];
+  const int n = t.n, w = t.ax_rows;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double* Y = const_cast<double*>(a.ypool) + t.ax_off;
+  __shared__ int s_ktol;
+  if (threadIdx.x == 0) {
+    const int mn_eff = gs[b].stop;
+    const double tol = a.rel_tol * fabs(Y[0]);
+    int kt = 0;
+    for (int i = 0; i < mn_eff; ++i) kt += fabs(Y[i + (int64_t)i * w]) > tol;
+    int kmax = a.kmax;
+    if (kmax == 0 || kmax > n) kmax = n;
+    gs[b].ktol = kt;
+    gs[b].k = (n == 0 || w > kWMaxRows) ? 0 : min(kt, kmax);
+    s_ktol = kt;
+  }
+  __syncthreads();
+  const int ktol = s_ktol;
+  for (int c = wid; c < min(ktol, n); c += kWWarps)
+    for (int r = c + 1 + lane; r < ktol; r += 32) Y[r + (int64_t)c * w] = 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_gw_tsolve(CompressArgs a, GwState* gs) {
+  const int b = blockIdx.y;
+  const CompressTask t = a.tasks[b];
+  const int n = t.n, w = t.ax_rows, k = gs[b].k;
+  const int c = k + blockIdx.x * 256 + threadIdx.x;
+  if (k <= 0 || c >= n) return;
+  const double* Y = a.ypool + t.ax_off;
+  auto y = [&](int r, int cc) { return Y[r + (int64_t)cc * w]; };
+  double* yc = const_cast<double*>(Y) + (int64_t)c * w;
+  for (int i1 = k; i1 > 0;) {
+    const int i0 = i1 > 32 ? i1 - 32 : 0, bs = i1 - i0;
+    double x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = j < bs ? yc[i0 + j] : 0.0;
+#pragma unroll
+    for (int j = 31; j >= 0; --j) {
+      if (j < bs) {
+        double vv = x[j];
+#pragma unroll
+        for (int l = j + 1; l < 32; ++l)
+          if (l < bs) vv -= y(i0 + j, i0 + l) * x[l];
+        x[j] = vv / y(i0 + j, i0 + j);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (j < bs) yc[i0 + j] = x[j];
+    for (int rr = 0; rr < i0; ++rr) {
+      double vv = yc[rr];
+      const double* Rr = Y + rr + (int64_t)i0 * w;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < bs) vv -= Rr[(int64_t)j * w] * x[j];
+      yc[rr] = vv;
+    }
+    i1 = i0;
+  }
+}
+
+__global__ void __launch_bounds__(kWThreads) k_gw_out(CompressArgs a, GwState* gs) {
+  __shared__ double red[kWWarps];
+  __shared__ int s_k;
+  const int b = blockIdx.x;
+  const CompressTask t = a.tasks[b];
+  const int n = t.n, w = t.ax_rows;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  CompressOut* out = a.out + t.out_idx;
+  if (n == 0 || w > kWMaxRows) {
+    if (tid == 0) *out = CompressOut{0, 0, 0, n == 0 ? 0 : (int)ST_ID_CHECK};
+    return;
+  }
+  double* Y = const_cast<double*>(a.ypool) + t.ax_off;
+  auto y = [&](int r, int c) -> double& { return Y[r + (int64_t)c * w]; };
+  double* vn1 = a.scratch + t.scr_off;
+  double* aux = vn1 + 2 * (int64_t)n;
+  int* jpvt = reinterpret_cast<int*>(aux + 6 * (int64_t)n);
+  int64_t* slf = a.ipool + t.slf_off;
+  int k = gs[b].k;
+  const int ktol = gs[b].ktol;
+  if (tid == 0) s_k = k;
+  if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
+    double mx = 0.0;
+    for (int c = k + tid; c < n; c += kWThreads)
+      for (int i = 0; i < k; ++i) mx = fmax(mx, y(i, c) * y(i, c));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[wid] = mx;
+    __syncthreads();
+    if (tid == 0) {
+      double bm = 0.0;
+      for (int q = 0; q < kWWarps; ++q) bm = fmax(bm, red[q]);
+      if (ktol > k || bm > a.Tmax * a.Tmax) {
+        int niter = 0, capped = 0;
+        const double tol = a.rel_tol * fabs(y(0, 0));
+        s_k = rrqr_serial(Y, 1, w, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped);
+        gs[b].niter = niter;
+        gs[b].cap = capped;
+      }
+    }
+  }
+  __syncthreads();
+  k = s_k;
+  const int r = n - k;
+  int* perm_out = a.permpool + t.perm_off;
+  int64_t* tmp_ids = reinterpret_cast<int64_t*>(aux);
+  for (int q = tid; q < n; q += kWThreads) tmp_ids[q] = slf[q];
+  __syncthreads();
+  for (int q = tid; q < n; q += kWThreads) {
+    const int src = r == 0 ? q : jpvt[q];
+    perm_out[q] = src;
+    slf[q] = tmp_ids[src];
+  }
+  if (r > 0 && k > 0) {
+    double* T = a.tpool + t.T_off;
+    for (int c = k + wid; c < n; c += kWWarps)
+      for (int i = lane; i < k; i += 32) T[i + (int64_t)(c - k) * k] = y(i, c);
+  }
+  if (tid == 0) {
+    int st = gs[b].cap ? (int)ST_RRQR_CAP : 0;
+    if (k > w - t.ax_guard) st |= ST_ID_CHECK;
+    *out = CompressOut{k, w, gs[b].niter, st};
+  }
+}
+
 }  // namespace
 
 int64_t cpqr_wide_scratch_doubles(int n) { return 8 * (int64_t)n + n / 2 + 2; }
@@ -273,6 +560,22 @@ int64_t cpqr_wide_scratch_doubles(int n) { return 8 * (int64_t)n + n / 2 + 2; }
 void launch_cpqr_wide(const CompressArgs& a, int ntask, cudaStream_t s) {
   if (ntask <= 0) return;
   k_cpqr_wide<<<ntask, kWThreads, 0, s>>>(a);
+}
+
+size_t cpqr_grid_state_bytes(int ntask) { return sizeof(GwState) * (size_t)std::max(ntask, 1); }
+
+void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int steps, void* state, cudaStream_t s) {
+  if (ntask <= 0) return;
+  GwState* gs = static_cast<GwState*>(state);
+  const unsigned cb = (unsigned)((nmax + kWWarps - 1) / kWWarps), z = (unsigned)ntask;
+  k_gw_norms<<<dim3(cb, z), kWThreads, 0, s>>>(a, gs);
+  for (int i = 0; i < steps; ++i) {
+    k_gw_pivot<<<z, kWThreads, 0, s>>>(a, gs, i);
+    k_gw_apply<<<dim3(cb, z), kWThreads, 0, s>>>(a, gs, i);
+  }
+  k_gw_rank<<<z, kWThreads, 0, s>>>(a, gs);
+  k_gw_tsolve<<<dim3((unsigned)((nmax + 255) / 256), z), 256, 0, s>>>(a, gs);
+  k_gw_out<<<z, kWThreads, 0, s>>>(a, gs);
 }
 
 }  // namespace flam

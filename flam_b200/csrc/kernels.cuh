@@ -45,6 +45,11 @@ void launch_compress_tc(const CompressArgs& a, int ntask, int nt, int b, int g, 
 // per box; scratch: cpqr_wide_scratch_doubles(n) at the task's scr_off.
 int64_t cpqr_wide_scratch_doubles(int n);
 void launch_cpqr_wide(const CompressArgs& a, int ntask, cudaStream_t s);
+// The same with every pivot step spread over the GPU (fewer wide boxes than SMs): 2 launches per step
+// for `steps` steps (>= min(rows, n) of every task), per-task state of
+// cpqr_grid_state_bytes(ntask) bytes in device memory.
+size_t cpqr_grid_state_bytes(int ntask);
+void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int steps, void* state, cudaStream_t s);
 // Neighbour filter alone (row-split form): tasks[0, ntask) compact their candidates
 // and write the kept count to a.mfilt[out_idx].
 void launch_filter(const CompressArgs& a, int ntask, cudaStream_t s);

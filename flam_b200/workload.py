@@ -1,41 +1,68 @@
-"""One factor + solve of the star-curve workload, for profilers.
+"""One factor + solve of a benchmark workload, for kernel profilers.
 
-    python -m flam_b200.workload [--n 65536] [--nrhs 16] [--reps 1] [--symm n]
+    python -m flam_b200.workload [--cfg star|sphere] [--n 65536] [--nrhs 16] [--reps 1]
+                                 [--form plain|chosen] [--symm n] [--tol 1e-10]
 
-Runs ``reps`` factorizations and solves of the Beta-clustered star curve
-(the benchmark's geometry and matrix at a chosen size) on cuda:0 with no
-warm-up and nothing else launched, so a kernel profiler sees only the
-factorization's and the sweeps' kernels.
+Runs ``reps`` factorizations and solves on cuda:0 with no warm-up and nothing else
+launched, so a kernel profiler sees only the library's kernels:
+
+* ``--form plain``: the exact ID at ``--tol`` and rskelf_sv;
+* ``--form chosen``: the sketched factorization at tol 1e-6 with the trained rank
+  predictor (flam_b200/predictor_weights.npz) and FP64 refinement to 1e-10, whose
+  residual steps are the on-the-fly FP64 matvec.
+
+``--cfg star`` is the Beta-clustered star curve of the benchmark (2D log kernel);
+``--cfg sphere`` the Fibonacci sphere of the mixed-precision configuration (3D Laplace,
+256-point proxy sphere).  This is the entry point the committed ncu summaries name.
 """
 import argparse
+import os
 
 import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--cfg", default="star", choices=["star", "sphere"])
     ap.add_argument("--n", type=int, default=65536)
     ap.add_argument("--nrhs", type=int, default=16)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--symm", default="n")
     ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--form", default="plain", choices=["plain", "chosen"])
     args = ap.parse_args()
     import torch
 
     import flam_b200 as fb
     from flam_b200 import problems
 
-    x, A, pxy = problems.star(args.n, seed=0)
+    if args.cfg == "star":
+        x, A, pxy = problems.star(args.n, seed=0)
+    else:
+        x, A, pxy = problems.sphere(args.n, p=256, seed=0)
     xd = torch.from_numpy(np.ascontiguousarray(x.T)).cuda().t()
-    Ad = fb.Kernel(A.kind, scale=A.scale, dval=A.dval, weights=torch.from_numpy(A.weights).cuda())
+    w = None if A.weights is None else torch.from_numpy(A.weights).cuda()
+    Ad = fb.Kernel(A.kind, scale=A.scale, dval=A.dval, param=A.param, weights=w)
     B = torch.randn(args.n, args.nrhs, dtype=torch.float64, device="cuda").t().contiguous().t()
+    pred = None
+    if args.form == "chosen":
+        pred = fb.Predictor.load(os.path.join(HERE, "predictor_weights.npz"))
     for _ in range(args.reps):
-        F = fb.rskelf(Ad, xd, 64, args.tol, pxy, dict(symm=args.symm))
-        X = B.clone()
-        F.sv_(X)
+        if args.form == "plain":
+            F = fb.rskelf(Ad, xd, 64, args.tol, pxy, dict(symm=args.symm))
+            X = B.clone()
+            F.sv_(X)
+            extra = ""
+        else:
+            F = fb.rskelf(Ad, xd, 64, 1e-6, pxy, dict(symm=args.symm, sketch=1, predictor=pred, sketch_p=12))
+            X = torch.empty_like(B)
+            _, it, rel = F.ir_sv_(B, X, 1e-10, 10)
+            extra = f" refinement steps {it} relres {float(np.max(rel)):.2e}"
         torch.cuda.synchronize()
         F.free()
-    print("ok", args.n, args.nrhs, args.reps)
+    print("ok", args.cfg, args.form, args.n, args.nrhs, args.reps, extra)
 
 
 if __name__ == "__main__":

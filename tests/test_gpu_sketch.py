@@ -108,3 +108,25 @@ def test_autotune_records_a_setting_that_later_factorizations_use():
     assert np.all(np.abs(sf[:, 3] - sg[:, 3]) <= 0.002 * sg[:, 3] + 1)
     with pytest.raises(fb.FlamError, match="tune:invalidArg"):
         fb.tune_set(2, "laplace2d", 20000, dict(split_ctas=0, split_max=8, split_min_n=32, tc_smem_max=0))
+
+
+def test_low_sketch_widths_on_wide_boxes_take_a_second_full_sketch():
+    """A box of more than 1024 points whose rank fills its sketch is sketched again at full
+    width (the adaptive fallback) instead of taking the exact per-column ID."""
+    import time
+    import torch
+    N = 16384
+    x, A, pxy = problems.sphere(N, p=256, seed=11)
+    t0 = time.time()
+    F = fb.rskelf(A, x, 64, 1e-6, pxy, dict(symm="n", sketch=1, sketch_p=-700, profile=True))
+    torch.cuda.synchronize()
+    dt = time.time() - t0
+    prof = F.profile()
+    assert prof["n_sketch_redo"] > 0
+    assert dt < 20.0, dt
+    B = torch.randn(N, 2, dtype=torch.float64, device="cuda").t().contiguous().t()
+    X = torch.empty_like(B)
+    _, it, rel = F.ir_sv_(B, X, 1e-10, 10)
+    R = torch.empty_like(B)
+    F.matvec_(X, R, B)
+    assert (R.norm(dim=0) / B.norm(dim=0)).max().item() <= 1e-10
