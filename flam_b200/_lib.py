@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libflam_b200.so")
 FLAM_OK = 0
 STATUS = {
     0: "FLAM_OK", 1: "FLAM_ERR_ARG", 2: "FLAM_ERR_NOT_SPD", 3: "FLAM_ERR_CUDA", 4: "FLAM_ERR_NOMEM",
-    5: "FLAM_ERR_UNSUPPORTED", 6: "FLAM_ERR_TIMEOUT", 7: "FLAM_ERR_ID_CHECK",
+    5: "FLAM_ERR_UNSUPPORTED", 6: "FLAM_ERR_TIMEOUT",
     100: "FLAM_WARN_RRQR_MAXITER", 101: "FLAM_WARN_SINGULAR", 102: "FLAM_WARN_IR_NOT_CONVERGED",
 }
 
@@ -65,7 +65,8 @@ class FlamProf(C.Structure):
                 ("t_compress", C.c_double), ("t_elim", C.c_double), ("t_sweep", C.c_double),
                 ("flop_compress", C.c_double), ("flop_elim", C.c_double), ("flop_sweep", C.c_double),
                 ("byte_sweep", C.c_double), ("n_sketch", C.c_int64), ("n_sketch_redo", C.c_int64),
-                ("sketch_rows", C.c_int64), ("sketch_rows_k", C.c_int64), ("id_rows", C.c_int64)]
+                ("sketch_rows", C.c_int64), ("sketch_rows_k", C.c_int64), ("id_rows", C.c_int64),
+                ("graph_replays", C.c_int64)]
 
 
 class FlamError(RuntimeError):

@@ -189,6 +189,7 @@ struct Workspace {
   DBuf<float> feat, fyhat;
   DBuf<double> irB, irX, irR, irW, colsq;
   cudaStream_t copy = nullptr;   // host<->device copies overlapped with the sweeps
+  cudaStream_t cap = nullptr;    // stream the sweep graphs are captured on
   // side streams for the independent launches of one step (the kernel shapes of a
   // compress segment, the two elimination kernels): forked from the step's stream
   // by one event and joined back by one event each
@@ -235,6 +236,10 @@ struct Workspace {
     }
   }
   void release(cudaStream_t s) {
+    if (cap) {
+      cudaStreamDestroy(cap);
+      cap = nullptr;
+    }
     if (copy) {
       cudaStreamSynchronize(copy);
       cudaStreamDestroy(copy);
@@ -381,6 +386,23 @@ struct flam_factor {
   std::vector<float> rlog_X, rlog_y;   // opts.rank_log: features and k/n of every compressed box
   bool profile = false;
   mutable flam_prof prof{};
+  // CUDA graphs of the sweep launches of an apply, by (X, ld, nrhs, trans, solve, halves,
+  // work array): the second apply with the same key captures, later ones replay
+  struct GraphKey {
+    const void* X;
+    int64_t ld, nrhs;
+    int t, solve, halves;
+    const void* W;
+    bool operator<(const GraphKey& o) const {
+      return std::tie(X, ld, nrhs, t, solve, halves, W) < std::tie(o.X, o.ld, o.nrhs, o.t, o.solve, o.halves, o.W);
+    }
+  };
+  struct GraphRec {
+    cudaGraphExec_t exec;
+    flam_prof delta;   // the accounting of one apply's launches
+  };
+  mutable std::map<GraphKey, GraphRec> graphs;
+  mutable std::map<GraphKey, int> graph_seen;
   mutable cudaEvent_t pend[2] = {nullptr, nullptr};   // sweep timing not yet read
   mutable bool has_pend = false;
   void resolve_pending() const {
@@ -395,6 +417,7 @@ struct flam_factor {
 
   ~flam_factor() {
     resolve_pending();
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second.exec);
     const bool any = x.p || ipool.p || fpool.p || ppool.p || hperm.p || ip.p || !steps.empty();
     if (!any) return;   // nothing on the device (e.g. a handle that failed before its uploads)
     cudaStream_t st = s;
@@ -1800,6 +1823,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   CK(cudaStreamSynchronize(s));
   if (st & ST_NOT_SPD)
     fail(FLAM_ERR_NOT_SPD, "FLAM:rskelf:notPosDef: a redundant block is not positive definite (chol failed)");
+  if (st & ST_TIMEOUT)
+    fail(FLAM_ERR_TIMEOUT, "FLAM:gpu:timeout: a tensor-core sketch did not complete within its wait limit");
   if (st & ST_SINGULAR) F.warn |= 2;
   ws.hint_ipool = std::max(ws.hint_ipool, F.ipool.n);
   ws.hint_fpool = std::max(ws.hint_fpool, F.fpool.n);
@@ -1996,6 +2021,48 @@ void sweeps_on_device(const flam_factor* F, double* Xd, int64_t ld, int64_t nrhs
   launch_from_pointmajor(Wp, N, (int)nrhs, Xd, ld, s);
 }
 
+// The sweeps of an apply as a CUDA graph.  Once a factorization exists its apply is a
+// fixed launch sequence (layout change, one sweep launch per step and direction, layout
+// change), so the second apply on the same device buffers and shape captures it (on a
+// workspace stream, so that the caller's stream may be the legacy default stream) and
+// every later one replays it with one launch.  Returns false when the caller should run
+// the launches itself (first sighting, or a step whose sweep allocates scratch).
+bool apply_graph(const flam_factor* F, double* Xd, int64_t ld, int64_t nrhs, double* Wp, int t, bool solve,
+                 int halves, cudaStream_t s) {
+  const flam_factor::GraphKey key{Xd, ld, nrhs, t, solve ? 1 : 0, halves, Wp};
+  auto it = F->graphs.find(key);
+  if (it == F->graphs.end()) {
+    if (F->graph_seen[key]++ == 0) return false;
+    for (const StepDev& sd : F->steps)
+      if (!sweep_in_smem(sd.kmax, sd.rmax, solve ? 0 : 2)) return false;
+    Workspace& ws = workspace(F->dev, s);
+    if (!ws.cap) CK(cudaStreamCreateWithFlags(&ws.cap, cudaStreamNonBlocking));
+    const flam_prof before = F->prof;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ws.cap, cudaStreamCaptureModeThreadLocal));
+    sweeps_on_device(F, Xd, ld, nrhs, Wp, t, solve, halves, ws.cap);
+    CK(cudaStreamEndCapture(ws.cap, &g));
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CK(ei);
+    flam_factor::GraphRec rec{ex, {}};
+    rec.delta.launches = F->prof.launches - before.launches;
+    rec.delta.n_sweep = F->prof.n_sweep - before.n_sweep;
+    rec.delta.flop_sweep = F->prof.flop_sweep - before.flop_sweep;
+    rec.delta.byte_sweep = F->prof.byte_sweep - before.byte_sweep;
+    F->prof = before;
+    it = F->graphs.emplace(key, rec).first;
+  }
+  CK(cudaGraphLaunch(it->second.exec, s));
+  F->prof.launches += it->second.delta.launches;
+  F->prof.n_sweep += it->second.delta.n_sweep;
+  F->prof.flop_sweep += it->second.delta.flop_sweep;
+  F->prof.byte_sweep += it->second.delta.byte_sweep;
+  F->prof.graph_replays += 1;
+  return true;
+}
+
 // Apply with X in host memory: the right-hand sides go in two column halves whose
 // host->device copy, sweeps and device->host copy overlap (the copies run on the
 // workspace's copy stream, ordered by events).  Pinned X gives the overlap; pageable X
@@ -2083,6 +2150,11 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   } release_own{{&own_tmp, &own_W, &own_Y}, s};
   auto& tmp = own ? own_tmp : ws.tmp;
   auto& W = own ? own_W : ws.W;
+  if (dev && !fn && !pp && !F->profile) {
+    F->resolve_pending();
+    W.ensure(N * nrhs, s);
+    if (apply_graph(F, Xd, ld, nrhs, W.p, t, solve, halves, s)) return FLAM_OK;
+  }
   if (!dev) {
     tmp.ensure(N * nrhs, s);
     CK(cudaMemcpy2DAsync(tmp.p, sizeof(double) * N, X, sizeof(double) * ldx, sizeof(double) * N, nrhs,

@@ -812,6 +812,114 @@ __global__ void __launch_bounds__(kPanelThreads) k_hb_panel(ElimArgs a, int j0) 
   }
 }
 
+// The same LU panel spread over P CTAs per box (one cooperative launch, so every CTA is
+// resident): CTA `part` owns a contiguous block of the panel's rows.  Per column: local
+// pivot search, box barrier, the first CTA swaps the two rows inside the panel and records
+// the pivot, box barrier, every CTA scales and updates its rows.  The barriers are bounded
+// (2 s): on expiry the kernel flags the timeout status and returns.
+struct PanelSync {
+  unsigned count, gen;
+};
+struct PanelSlot {
+  double v;
+  int i, pad;
+};
+constexpr int kCoopThreads = 256;
+
+__device__ __forceinline__ uint64_t el_globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ bool box_barrier(PanelSync* ps, int P, int32_t* status) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+    volatile unsigned* vgen = &ps->gen;
+    const unsigned g = *vgen;
+    __threadfence();
+    if (atomicAdd(&ps->count, 1u) == (unsigned)P - 1) {
+      ps->count = 0;
+      __threadfence();
+      atomicAdd(&ps->gen, 1u);
+    } else {
+      const uint64_t t0 = el_globaltimer();
+      while (*vgen == g) {
+        if (el_globaltimer() - t0 > 2000000000ull) {
+          atomicOr(status, (int)ST_TIMEOUT);
+          s_ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(kCoopThreads) k_hb_panel_coop(ElimArgs a, int j0, int P, PanelSync* sync,
+                                                                PanelSlot* slots) {
+  constexpr int kW = kCoopThreads / 32;
+  __shared__ AM red[kW];
+  const int bx = blockIdx.x / P, part = blockIdx.x % P;
+  const ElimTask t = a.tasks[bx];
+  const int n = t.n, k = t.k, r = n - k;
+  if (r <= 0 || j0 >= r) return;   // uniform over the box's CTAs
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double* K = a.scratch + t.scr_off;
+  int* piv = reinterpret_cast<int*>(K + (int64_t)n * n) + 2 * n;
+  double* Kr = K + k + (int64_t)k * n;
+  auto kr = [&](int i, int j) -> double& { return Kr[i + (int64_t)j * n]; };
+  // other CTAs write the panel (the row swap, their rows): read it past L1
+  auto ld = [&](int i, int j) { return __ldcg(&Kr[i + (int64_t)j * n]); };
+  const int jb = min(kHb, r - j0), j1 = j0 + jb;
+  const int rb = j0 + (int)((int64_t)(r - j0) * part / P), re = j0 + (int)((int64_t)(r - j0) * (part + 1) / P);
+  PanelSync* ps = sync + bx;
+  PanelSlot* sl = slots + (int64_t)bx * P;
+  for (int j = j0; j < j1; ++j) {
+    AM am{-1.0, r};
+    for (int q = max(j, rb) + tid; q < re; q += kCoopThreads) am = amax(am, AM{fabs(ld(q, j)), q});
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      AM bb{__shfl_xor_sync(0xffffffffu, am.v, o), __shfl_xor_sync(0xffffffffu, am.i, o)};
+      am = amax(am, bb);
+    }
+    if (lane == 0) red[wid] = am;
+    __syncthreads();
+    if (tid == 0) {
+      AM bm = red[0];
+      for (int w = 1; w < kW; ++w) bm = amax(bm, red[w]);
+      sl[part] = PanelSlot{bm.v, bm.i, 0};
+    }
+    if (!box_barrier(ps, P, a.status)) return;
+    AM bm{-1.0, r};
+    for (int p = 0; p < P; ++p) {
+      volatile PanelSlot* vp = sl + p;   // written by other CTAs before the barrier
+      bm = amax(bm, AM{vp->v, vp->i});
+    }
+    const int pv = (bm.i >= j && bm.i < r) ? bm.i : j;
+    if (part == 0) {
+      if (pv != j && tid < jb) {
+        const double x = ld(j, j0 + tid);
+        kr(j, j0 + tid) = ld(pv, j0 + tid);
+        kr(pv, j0 + tid) = x;
+      }
+      if (tid == 0) piv[j] = pv;
+    }
+    if (!box_barrier(ps, P, a.status)) return;
+    const double dj = ld(j, j);
+    if (dj == 0.0 && part == 0 && tid == 0) atomicOr(a.status, (int)ST_SINGULAR);
+    for (int q = max(j + 1, rb) + tid; q < re; q += kCoopThreads) {
+      const double lq = dj != 0.0 ? ld(q, j) / dj : ld(q, j);
+      kr(q, j) = lq;
+      for (int c = j + 1; c < j1; ++c) kr(q, c) = ld(q, c) - lq * ld(j, c);
+    }
+  }
+}
+
 // The panel's row interchanges on every column of K(rd,:) outside the panel.
 __global__ void __launch_bounds__(kThreads) k_hb_swap(ElimArgs a, int j0) {
   const ElimTask t = a.tasks[blockIdx.z];
@@ -945,9 +1053,37 @@ void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int 
     gemm(HB_TCOL, 0, nmax, rmax);
   }
   const bool chol = a.symm == 'p';
+  // LU panels over several CTAs per box when the redundant blocks are tall (one CTA
+  // streams an r x 32 panel through its SM 32 times); all CTAs resident: one cooperative
+  // launch of at most one CTA per SM
+  int P = 1;
+  PanelSync* psync = nullptr;
+  PanelSlot* pslot = nullptr;
+  if (!chol && rmax >= 1024) {
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    P = std::max(1, std::min(64, nsm / nbox));
+    if (P > 1 && (cudaMallocAsync(&psync, sizeof(PanelSync) * nbox, s) != cudaSuccess ||
+                  cudaMallocAsync(&pslot, sizeof(PanelSlot) * nbox * P, s) != cudaSuccess)) {
+      cudaGetLastError();
+      P = 1;
+    }
+    if (P > 1) cudaMemsetAsync(psync, 0, sizeof(PanelSync) * nbox, s);
+  }
   for (int j0 = 0; j0 < rmax; j0 += kHb) {
     const int rest = rmax - std::min(rmax, j0 + kHb);
-    k_hb_panel<<<nbox, kPanelThreads, 0, s>>>(a, j0);
+    bool done = false;
+    if (P > 1) {
+      ElimArgs ac = a;
+      int jj = j0, pp = P;
+      void* args[] = {&ac, &jj, &pp, &psync, &pslot};
+      if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_hb_panel_coop), dim3((unsigned)(nbox * P)),
+                                      dim3(kCoopThreads), args, 0, s) == cudaSuccess)
+        done = true;
+      else
+        cudaGetLastError();   // not resident together: the one-CTA panel
+    }
+    if (!done) k_hb_panel<<<nbox, kPanelThreads, 0, s>>>(a, j0);
     if (!chol) {
       k_hb_swap<<<dim3((nmax + kThreads - 1) / kThreads, 1, z), kThreads, 0, s>>>(a, j0);
       if (rest > 0) k_hb_trsm<<<dim3((rest + 127) / 128, 1, z), 128, 0, s>>>(a, j0, 0);
@@ -966,6 +1102,8 @@ void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int 
     }
     gemm(HB_SCHUR, 0, kmax, kmax);
   }
+  if (psync) cudaFreeAsync(psync, s);
+  if (pslot) cudaFreeAsync(pslot, s);
   const int64_t tot = 4 * (int64_t)std::max(kmax, 1) * rmax + (int64_t)rmax * rmax;
   k_hb_store<<<dim3((unsigned)std::min<int64_t>((tot + kThreads - 1) / kThreads, 4096), 1, z), kThreads, 0, s>>>(a);
 }

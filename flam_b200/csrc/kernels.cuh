@@ -105,6 +105,8 @@ struct SweepArgs {
   int symm;
 };
 void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t s);
+// Whether a step's sweep keeps its tiles in shared memory (otherwise it allocates scratch).
+bool sweep_in_smem(int kmax, int rmax, int op);
 
 // Layout changes for the user's column-major X (N x nrhs, ld) <-> point-major work array.
 void launch_to_pointmajor(const double* X, int64_t ld, int64_t N, int nrhs, double* W, cudaStream_t s);

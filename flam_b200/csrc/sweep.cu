@@ -345,6 +345,10 @@ void launch_rows_pm(double* W, int nrhs, const int64_t* idx, int64_t n, double* 
   k_rows_pm<<<g, dim3(32, 8), 0, s>>>(W, nrhs, idx, n, Y, dir);
 }
 
+bool sweep_in_smem(int kmax, int rmax, int op) {
+  return sizeof(double) * (size_t)((int64_t)(kmax + (op >= 2 ? 2 : 1) * rmax) * kTs) <= 200 * 1024;
+}
+
 void launch_sweep(const SweepArgs& a, int nfac, int kmax, int rmax, cudaStream_t s) {
   if (nfac <= 0 || a.nrhs <= 0) return;
   // X(sk), X(rd) and, for the multiplies, a scratch tile for the triangular

@@ -49,8 +49,7 @@ typedef enum {
   FLAM_ERR_CUDA = 3,         /* a CUDA runtime call failed */
   FLAM_ERR_NOMEM = 4,        /* device allocation failed */
   FLAM_ERR_UNSUPPORTED = 5,  /* option not available on the device path */
-  FLAM_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
-  FLAM_ERR_ID_CHECK = 7,     /* posterior ID residual check failed */
+  FLAM_ERR_TIMEOUT = 6,      /* a bounded device wait gave up (the sketch kernel's mbarrier) */
   FLAM_WARN_RRQR_MAXITER = 100, /* FLAM:id:maxIterCount (factor is still valid) */
   FLAM_WARN_SINGULAR = 101,     /* an LU pivot of a redundant block was exactly zero */
   FLAM_WARN_IR_NOT_CONVERGED = 102 /* refinement stopped above ir_tol (X is the last iterate) */
@@ -395,6 +394,7 @@ typedef struct {
   int64_t sketch_rows;     /* sum over the sketched boxes of their sketch rows w */
   int64_t sketch_rows_k;   /* sum over the same boxes of rows(K), the rows the exact ID folds */
   int64_t id_rows;         /* rows every ID of the factorization folded (w if sketched, else rows(K)) */
+  int64_t graph_replays;   /* applies run as a replayed CUDA graph of their sweep launches */
 } flam_prof;
 
 FLAM_API flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset);

@@ -130,3 +130,55 @@ def test_low_sketch_widths_on_wide_boxes_take_a_second_full_sketch():
     R = torch.empty_like(B)
     F.matvec_(X, R, B)
     assert (R.norm(dim=0) / B.norm(dim=0)).max().item() <= 1e-10
+
+
+def test_repeated_applies_replay_a_cuda_graph():
+    import torch
+    x, A, pxy = problems.star(8000, seed=12)
+    xo, Ao, po = configs.star(8000, seed=12)
+    F = fb.rskelf(A, x, 64, 1e-10, pxy, dict(symm="n"))
+    B = torch.randn(8000, 40, dtype=torch.float64, device="cuda").t().contiguous().t()
+    X = torch.empty_like(B)
+    outs = []
+    for _ in range(4):                      # eager, capture + replay, replay, replay
+        X.copy_(B)
+        F.sv_(X)
+        outs.append(X.clone())
+    assert F.profile()["graph_replays"] == 3
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+    D = Ao.dense()
+    r = np.linalg.norm(D @ outs[-1].cpu().numpy() - B.cpu().numpy()) / np.linalg.norm(B.cpu().numpy())
+    assert r < 1e-8
+    Y = B.clone()
+    F.mv_(Y)                                # another key: eager again
+    assert F.profile()["graph_replays"] == 3
+
+
+def test_two_host_threads_factor_on_one_device():
+    """Handles made concurrently from two host threads on one device (per-device kernel
+    attributes and per-stream workspaces) give the same factorizations as one thread."""
+    import threading
+    import torch
+    probs = [problems.star(6000, seed=20), problems.sphere(4000, p=128, seed=21)]
+    ref = [fb.rskelf(A, x, 64, 1e-8, pxy, dict(symm="n")).level_stats() for x, A, pxy in probs]
+    out = [None, None]
+    errs = []
+
+    def work(i):
+        try:
+            st = torch.cuda.Stream()
+            x, A, pxy = probs[i]
+            F = fb.rskelf(A, x, 64, 1e-8, pxy, dict(symm="n", stream=st.cuda_stream))
+            out[i] = F.level_stats()
+        except Exception as e:   # noqa: BLE001 - reported below
+            errs.append(e)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for a, b in zip(out, ref):
+        assert np.array_equal(a, b)
