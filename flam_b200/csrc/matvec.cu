@@ -194,7 +194,48 @@ __global__ void k_add_cols(double* X, int64_t ldx, const double* R, int64_t ldr,
   }
 }
 
+// out[c] = sum_i X(i, c) Y(i, c): one CTA per column.
+__global__ void k_coldot(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t N, double* out) {
+  __shared__ double red[32];
+  const double* x = X + (int64_t)blockIdx.x * ldx;
+  const double* y = Y + (int64_t)blockIdx.x * ldy;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < N; i += blockDim.x) s += x[i] * y[i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) out[blockIdx.x] = v;
+  }
+}
+
+// Y(:, c) = a[c] Y(:, c) + b[c] X(:, c) (a == null: 1).
+__global__ void k_axpby_cols(double* Y, int64_t ldy, const double* X, int64_t ldx, const double* a, const double* b,
+                             int64_t N, int nrhs) {
+  const int64_t total = N * nrhs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e / N, i = e % N;
+    const double ya = a ? a[c] * Y[i + c * ldy] : Y[i + c * ldy];
+    Y[i + c * ldy] = ya + b[c] * X[i + c * ldx];
+  }
+}
+
 }  // namespace
+
+void launch_coldot(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t N, int nrhs, double* out,
+                   cudaStream_t s) {
+  if (nrhs <= 0) return;
+  k_coldot<<<nrhs, 256, 0, s>>>(X, ldx, Y, ldy, N, out);
+}
+
+void launch_axpby_cols(double* Y, int64_t ldy, const double* X, int64_t ldx, const double* a, const double* b, int64_t N,
+                       int nrhs, cudaStream_t s) {
+  if (N <= 0 || nrhs <= 0) return;
+  const int64_t blocks = std::min<int64_t>((N * nrhs + 255) / 256, 148 * 16);
+  k_axpby_cols<<<(unsigned)blocks, 256, 0, s>>>(Y, ldy, X, ldx, a, b, N, nrhs);
+}
 
 void launch_add_cols(double* X, int64_t ldx, const double* R, int64_t ldr, int64_t N, int nrhs, cudaStream_t s) {
   if (N <= 0 || nrhs <= 0) return;

@@ -29,6 +29,12 @@ int matvec_tile_cols(int nrhs);
 void launch_matvec(const MatvecArgs& a, int ntile, cudaStream_t s);
 // out[c] = sum_i Y(i, c)^2 for c < nrhs.
 void launch_add_cols(double* X, int64_t ldx, const double* R, int64_t ldr, int64_t N, int nrhs, cudaStream_t s);
+// out[c] = X(:, c) . Y(:, c) for c < nrhs.
+void launch_coldot(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t N, int nrhs, double* out,
+                   cudaStream_t s);
+// Y(:, c) = a[c] Y(:, c) + b[c] X(:, c), with a = null meaning 1 (a, b: device arrays).
+void launch_axpby_cols(double* Y, int64_t ldy, const double* X, int64_t ldx, const double* a, const double* b, int64_t N,
+                       int nrhs, cudaStream_t s);
 void launch_colsq(const double* Y, int64_t N, int64_t ld, int nrhs, double* out, cudaStream_t s);
 
 }  // namespace flam

@@ -264,6 +264,9 @@ FLAM_API flam_status flam_matvec(const flam_factor* F, const double* X, int64_t 
 /* X = A \ B by iterative refinement on the factorization F of A: X = F \ B
  * (rskelf_sv), then X += F \ (B - A X) with the FP64 residual of flam_matvec
  * until max_j ||B_j - A X_j|| / ||B_j|| <= ir_tol or max_iter refinement steps.
+ * For symm 'p' (A and F positive definite) the steps are conjugate gradients
+ * preconditioned by F, which also converge when A's conditioning spreads the
+ * spectrum of F \ A beyond what stationary refinement contracts.
  * F may be a loose (larger rank_or_tol) factorization; the returned error is the
  * FP64 relative residual per column (relres, nrhs entries, may be NULL), and
  * *iters the refinement steps taken.  FLAM_WARN_IR_NOT_CONVERGED when the

@@ -89,3 +89,18 @@ def test_refinement_rejects_imported_factors_and_reports_non_convergence():
     G = fb.factor_import(fac)
     with pytest.raises(fb.FlamError, match="noMatrix"):
         fb.matvec(G, B)
+
+
+def test_refinement_of_an_ill_conditioned_spd_matrix_converges():
+    """Matern-3/2 covariance with a 1e-2 nugget (cond ~ 1e4): from a loose factorization the
+    conjugate-gradient refinement of symm 'p' reaches 1e-10 where the stationary step would
+    not contract."""
+    x, A, pxy = problems.matern_cube(4000, seed=5, p=32, p_rad=4)
+    xo, Ao, po = configs.matern_cube(4000, seed=5, p=32, p_rad=4)
+    D = Ao.dense()
+    F = fb.rskelf(A, x, 64, 1e-5, pxy, dict(symm="p", sketch=1))
+    B = np.asfortranarray(np.random.default_rng(6).standard_normal((4000, 3)))
+    X, it, rel = fb.rskelf_ir_sv(F, B, ir_tol=1e-10, max_iter=30)
+    r = np.linalg.norm(D @ X - B, axis=0) / np.linalg.norm(B, axis=0)
+    assert r.max() <= 1e-10 and it <= 30
+    np.testing.assert_allclose(rel, r, rtol=1e-2, atol=1e-16)
