@@ -151,6 +151,41 @@ struct StepDev {
   double flop_per_rhs = 0;   // sum over factors of 4kr + r^2 (one direction, one right-hand side)
   double fac_bytes = 0;      // sum of 8 (2kr + r^2): factor data one direction reads
   double x_rows = 0;         // sum of k + r
+  // Factors with no skeletons and r >= kRootGridR (the root of a problem that stops
+  // with a large block): the solve sweeps run them grid-wide (sweep_root_grid) and the
+  // per-box sweep kernel takes the rest, listed in sfac with maxima skmax / srmax.
+  std::vector<FacDesc> roots;
+  DBuf<FacDesc> sfac;
+  int nsfac = 0, skmax = 0, srmax = 0;
+
+  // Fill from the step's factor list (in hfac order: the log-determinant indexes by it).
+  void set(const std::vector<FacDesc>& fd, cudaStream_t s) {
+    fac.upload(fd, s);
+    nfac = (int)fd.size();
+    std::vector<FacDesc> rest;
+    for (const FacDesc& f : fd) {
+      const double k = f.k, r = f.r;
+      kmax = std::max(kmax, f.k);
+      rmax = std::max(rmax, f.r);
+      flop_per_rhs += 4 * k * r + r * r;
+      fac_bytes += 8 * (2 * k * r + r * r);
+      x_rows += k + r;
+      if (f.k == 0 && f.r >= kRootGridR) {
+        roots.push_back(f);
+      } else {
+        rest.push_back(f);
+        skmax = std::max(skmax, f.k);
+        srmax = std::max(srmax, f.r);
+      }
+    }
+    if (!roots.empty()) sfac.upload(rest, s);
+    nsfac = (int)rest.size();
+  }
+  int root_rmax() const {
+    int m = 0;
+    for (const FacDesc& f : roots) m = std::max(m, f.r);
+    return m;
+  }
 };
 
 struct LevelStat {
@@ -369,6 +404,7 @@ struct flam_factor {
   DBuf<double> fpool;
   DBuf<int32_t> ppool;
   std::vector<StepDev> steps;
+  int root_rmax = 0;   // largest r of a grid-swept root factor (its r x nrhs scratch follows W)
   std::vector<HostFac> hfac;
   std::vector<std::vector<int64_t>> inst_fac;     // per instance: indices into hfac
   std::vector<std::vector<int64_t>> inst_lvp;     // per instance F.lvp
@@ -1563,7 +1599,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     std::vector<FacDesc> fd;
     std::vector<BoxRec> brec;
     int64_t mtop = 0;
-    int kmx = 0, rmx = 0, nmax_e = 0;
+    int nmax_e = 0;
     const bool chol = F.symm == 'p';
     for (int q = 0; q < nb; ++q) {
       const int32_t b = boxes[q];
@@ -1602,8 +1638,6 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         F.hfac.push_back(h);
         fpool_top += 2 * kr + rr + (chol ? 0 : kr);
         ppool_top += chol ? 0 : r;
-        kmx = std::max(kmx, k);
-        rmx = std::max(rmx, r);
         F.rem[t.inst] -= r;
       } else {
         t.fac_off = -1;
@@ -1737,16 +1771,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       lrec.clear();
     }
     StepDev sd;
-    sd.fac.upload(fd, s);
-    sd.nfac = (int)fd.size();
-    sd.kmax = kmx;
-    sd.rmax = rmx;
-    for (const FacDesc& f : fd) {
-      const double k = f.k, r = f.r;
-      sd.flop_per_rhs += 4 * k * r + r * r;
-      sd.fac_bytes += 8 * (2 * k * r + r * r);
-      sd.x_rows += k + r;
-    }
+    sd.set(fd, s);
+    F.root_rmax = std::max(F.root_rmax, sd.root_rmax());
     F.steps.push_back(std::move(sd));
     // ---- host state for the next step (rskelf.m:245-261)
     for (int q = 0; q < nb; ++q) {
@@ -1983,6 +2009,35 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
 // Which halves of the sweeps an apply runs.
 enum : int { kUp = 1, kDown = 2, kBoth = 3 };
 
+// Doubles of the point-major work array of an apply: N x nrhs, then the r x nrhs block
+// of the largest grid-swept root factor.
+int64_t sweep_w_size(const flam_factor* F, int64_t nrhs) { return (F->Ntot + F->root_rmax) * nrhs; }
+
+// The sweep of one step in direction a.op (launches only): the per-box kernel over the
+// step's factors, except that a solve sweeps the large root factors grid-wide with the
+// scratch block rscr.
+void sweep_step(const flam_factor* F, const StepDev& sd, SweepArgs& a, double* rscr, cudaStream_t s) {
+  if (sd.nfac == 0) return;
+  const bool grid = !sd.roots.empty() && a.op <= 1;
+  if (grid) {
+    a.fac = sd.sfac.p;
+    launch_sweep(a, sd.nsfac, sd.skmax, sd.srmax, s);
+    F->prof.launches += sd.nsfac > 0;
+    for (const FacDesc& f : sd.roots) {
+      const int64_t* rd = F->ipool.p + f.sk_off;
+      F->prof.launches += sweep_root_grid(a.X, a.nrhs, rd, F->ppool.p + f.piv_off, F->fpool.p + f.LU_off, f.r, a.op,
+                                          a.trans, a.symm, rscr, s);
+    }
+  } else {
+    a.fac = sd.fac.p;
+    launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
+    F->prof.launches += 1;
+  }
+  F->prof.n_sweep += 1;
+  F->prof.flop_sweep += sd.flop_per_rhs * (double)a.nrhs;
+  F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)a.nrhs;
+}
+
 // The sweeps on a column-major device block Xd (N x nrhs, leading dimension ld), with the
 // point-major work array Wp (N x nrhs) -- launches only, on stream s.
 void sweeps_on_device(const flam_factor* F, double* Xd, int64_t ld, int64_t nrhs, double* Wp, int t, bool solve,
@@ -1999,16 +2054,8 @@ void sweeps_on_device(const flam_factor* F, double* Xd, int64_t ld, int64_t nrhs
   a.trans = t;
   a.symm = F->symm;
   const int ns = (int)F->steps.size();
-  auto sweep = [&](int q) {
-    const StepDev& sd = F->steps[q];
-    a.fac = sd.fac.p;
-    if (sd.nfac == 0) return;
-    launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
-    F->prof.launches += 1;
-    F->prof.n_sweep += 1;
-    F->prof.flop_sweep += sd.flop_per_rhs * (double)nrhs;
-    F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)nrhs;
-  };
+  double* rscr = Wp + N * nrhs;
+  auto sweep = [&](int q) { sweep_step(F, F->steps[q], a, rscr, s); };
   F->prof.launches += 2;
   if (halves & kUp) {
     a.op = solve ? 0 : 2;
@@ -2033,8 +2080,10 @@ bool apply_graph(const flam_factor* F, double* Xd, int64_t ld, int64_t nrhs, dou
   auto it = F->graphs.find(key);
   if (it == F->graphs.end()) {
     if (F->graph_seen[key]++ == 0) return false;
-    for (const StepDev& sd : F->steps)
-      if (!sweep_in_smem(sd.kmax, sd.rmax, solve ? 0 : 2)) return false;
+    for (const StepDev& sd : F->steps) {
+      const bool grid = !sd.roots.empty() && solve;
+      if (!sweep_in_smem(grid ? sd.skmax : sd.kmax, grid ? sd.srmax : sd.rmax, solve ? 0 : 2)) return false;
+    }
     Workspace& ws = workspace(F->dev, s);
     if (!ws.cap) CK(cudaStreamCreateWithFlags(&ws.cap, cudaStreamNonBlocking));
     const flam_prof before = F->prof;
@@ -2075,7 +2124,7 @@ flam_status apply_host_pipelined(const flam_factor* F, double* X, int64_t ldx, i
   if (!ws.copy) CK(cudaStreamCreateWithFlags(&ws.copy, cudaStreamNonBlocking));
   const cudaStream_t cs = ws.copy;
   ws.tmp.ensure(N * nrhs, s);
-  ws.W.ensure(N * nrhs, s);
+  ws.W.ensure(sweep_w_size(F, nrhs), s);
   constexpr int kChunks = 2;
   cudaEvent_t ev[2 * kChunks + 2];
   for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -2152,7 +2201,7 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   auto& W = own ? own_W : ws.W;
   if (dev && !fn && !pp && !F->profile) {
     F->resolve_pending();
-    W.ensure(N * nrhs, s);
+    W.ensure(sweep_w_size(F, nrhs), s);
     if (apply_graph(F, Xd, ld, nrhs, W.p, t, solve, halves, s)) return FLAM_OK;
   }
   if (!dev) {
@@ -2162,7 +2211,7 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
     Xd = tmp.p;
     ld = N;
   }
-  W.ensure(N * nrhs, s);
+  W.ensure(sweep_w_size(F, nrhs), s);
   mark(1);
   launch_to_pointmajor(Xd, ld, N, (int)nrhs, W.p, s);
   mark(2);
@@ -2187,9 +2236,9 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
   // FLAM_PROFILE: one event pair per sweep launch, printed with the step's shape
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sev;
   std::vector<int> sstep;
+  double* rscr = W.p + N * nrhs;
   auto sweep = [&](int q) {
     const StepDev& sd = F->steps[q];
-    a.fac = sd.fac.p;
     if (sd.nfac == 0) return;
     if (pp) {
       sev.emplace_back();
@@ -2198,12 +2247,8 @@ flam_status apply(const flam_factor* F, double* X, int64_t ldx, int64_t nrhs, ch
       CK(cudaEventRecord(sev.back().first, s));
       sstep.push_back(q);
     }
-    launch_sweep(a, sd.nfac, sd.kmax, sd.rmax, s);
+    sweep_step(F, sd, a, rscr, s);
     if (pp) CK(cudaEventRecord(sev.back().second, s));
-    F->prof.launches += 1;
-    F->prof.n_sweep += 1;
-    F->prof.flop_sweep += sd.flop_per_rhs * (double)nrhs;
-    F->prof.byte_sweep += sd.fac_bytes + 16.0 * sd.x_rows * (double)nrhs;
   };
   F->prof.launches += 2;  // layout changes
   if (halves & kUp) {
@@ -2372,7 +2417,7 @@ flam_status ir_solve(const flam_factor* F, const double* B, int64_t ldb, double*
     lx = N;
   }
   ws.irR.ensure(N * nrhs, s);
-  ws.W.ensure(N * nrhs, s);
+  ws.W.ensure(sweep_w_size(F, nrhs), s);
   ws.colsq.ensure(6 * nrhs, s);   // column norms and the conjugate-gradient coefficients
   double* R = ws.irR.p;
   // X = F \ B
@@ -3368,15 +3413,8 @@ flam_status flam_factor_import(int64_t N, char symm, int64_t nfac, const int64_t
     for (auto& grp : groups) {
       if (grp.empty()) continue;
       StepDev sd;
-      sd.fac.upload(grp, H->s);
-      sd.nfac = (int)grp.size();
-      for (const FacDesc& f : grp) {
-        sd.kmax = std::max(sd.kmax, f.k);
-        sd.rmax = std::max(sd.rmax, f.r);
-        sd.flop_per_rhs += 4.0 * f.k * f.r + (double)f.r * f.r;
-        sd.fac_bytes += 8.0 * (2.0 * f.k * f.r + (double)f.r * f.r);
-        sd.x_rows += f.k + f.r;
-      }
+      sd.set(grp, H->s);
+      H->root_rmax = std::max(H->root_rmax, sd.root_rmax());
       H->steps.push_back(std::move(sd));
       H->inst_lvp[0].push_back(H->inst_lvp[0].back() + (int64_t)grp.size());
     }

@@ -32,8 +32,68 @@ __device__ __forceinline__ WAm wbetter(WAm a, WAm b) {
   return a;
 }
 
+// T = R11 \ R12 in place for the columns c = k + c0 + tid (one per thread, c0 over
+// blockDim-wide groups), R11 (k x k, upper) and R12 in Y (ld w).  Back substitution by
+// 32-row blocks from the bottom; the block's diagonal part and, 64 rows at a time, the
+// part above it are staged in shared memory (coalesced loads, broadcast reads), so a
+// thread streams only its own column.  Called by every thread of the CTA.
+__device__ void tsolve_block_columns(double* Y, int w, int k, int n, int cfirst, int cstep, double* sd, double* su) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int cg = cfirst; cg < n - k; cg += cstep) {
+    const int c = k + cg + tid;
+    const bool live = c < n;
+    double* yc = Y + (int64_t)(live ? c : k) * w;
+    for (int i1 = k; i1 > 0;) {
+      const int i0 = i1 > 32 ? i1 - 32 : 0, bs = i1 - i0;
+      __syncthreads();
+      for (int e = tid; e < 32 * 32; e += nt) {   // sd[j * 33 + l] = R(i0 + j, i0 + l)
+        const int j = e % 32, l = e / 32;
+        sd[j * 33 + l] = (j < bs && l < bs) ? Y[(i0 + j) + (int64_t)(i0 + l) * w] : 0.0;
+      }
+      __syncthreads();
+      double x[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) x[j] = (live && j < bs) ? yc[i0 + j] : 0.0;
+#pragma unroll
+      for (int j = 31; j >= 0; --j) {
+        if (j < bs) {
+          double v = x[j];
+#pragma unroll
+          for (int l = j + 1; l < 32; ++l)
+            if (l < bs) v -= sd[j * 33 + l] * x[l];
+          x[j] = v / sd[j * 33 + j];
+        }
+      }
+      if (live) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (j < bs) yc[i0 + j] = x[j];
+      }
+      for (int r0 = 0; r0 < i0; r0 += 64) {
+        const int rn = min(64, i0 - r0);
+        __syncthreads();
+        for (int e = tid; e < 64 * 32; e += nt) {   // su[rr * 33 + j] = R(r0 + rr, i0 + j)
+          const int rr = e % 64, j = e / 64;
+          su[rr * 33 + j] = (rr < rn && j < bs) ? Y[(r0 + rr) + (int64_t)(i0 + j) * w] : 0.0;
+        }
+        __syncthreads();
+        if (live) {
+          for (int rr = 0; rr < rn; ++rr) {
+            double v = yc[r0 + rr];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v -= su[rr * 33 + j] * x[j];
+            yc[r0 + rr] = v;
+          }
+        }
+      }
+      i1 = i0;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
   __shared__ double vbuf[kWMaxRows];
+  __shared__ double tsd[32 * 33], tsu[64 * 33];
   __shared__ double red[kWWarps];
   __shared__ WAm ram[kWWarps];
   __shared__ int s_k, s_ktol, s_niter, s_cap, s_need, s_pvt, s_stop;
@@ -179,42 +239,8 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
   for (int c = wid; c < min(ktol, n); c += kWWarps)
     for (int r = c + 1 + lane; r < ktol; r += 32) y(r, c) = 0.0;
   __syncthreads();
-  // T = R11 \ R12, a thread per column, 32-row blocks from the bottom: the block's
-  // unknowns in registers (diagonal solve), then one pass over the rows above it
-  // (R's entries are the same for every thread: broadcast loads)
-  if (k > 0 && k < n) {
-    for (int c = k + tid; c < n; c += kWThreads) {
-      double* yc = &y(0, c);
-      for (int i1 = k; i1 > 0;) {
-        const int i0 = i1 > 32 ? i1 - 32 : 0, bs = i1 - i0;
-        double x[32];
-#pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = j < bs ? yc[i0 + j] : 0.0;
-#pragma unroll
-        for (int j = 31; j >= 0; --j) {
-          if (j < bs) {
-            double v = x[j];
-#pragma unroll
-            for (int l = j + 1; l < 32; ++l)
-              if (l < bs) v -= y(i0 + j, i0 + l) * x[l];
-            x[j] = v / y(i0 + j, i0 + j);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (j < bs) yc[i0 + j] = x[j];
-        for (int rr = 0; rr < i0; ++rr) {
-          double v = yc[rr];
-          const double* Rr = &y(rr, i0);
-#pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (j < bs) v -= Rr[(int64_t)j * w] * x[j];
-          yc[rr] = v;
-        }
-        i1 = i0;
-      }
-    }
-  }
+  // T = R11 \ R12 (shared-memory staged blocks)
+  if (k > 0 && k < n) tsolve_block_columns(Y, w, k, n, 0, kWThreads, tsd, tsu);
   __syncthreads();
   // RRQR refinement (id.m:117-236), on thread 0, when some |T| > Tmax or rows were cut
   if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
@@ -450,42 +476,13 @@ __global__ void __launch_bounds__(kWThreads) k_gw_rank(CompressArgs a, GwState* 
 }
 
 __global__ void __launch_bounds__(256) k_gw_tsolve(CompressArgs a, GwState* gs) {
+  __shared__ double tsd[32 * 33], tsu[64 * 33];
   const int b = blockIdx.y;
   const CompressTask t = a.tasks[b];
   const int n = t.n, w = t.ax_rows, k = gs[b].k;
-  const int c = k + blockIdx.x * 256 + threadIdx.x;
-  if (k <= 0 || c >= n) return;
-  const double* Y = a.ypool + t.ax_off;
-  auto y = [&](int r, int cc) { return Y[r + (int64_t)cc * w]; };
-  double* yc = const_cast<double*>(Y) + (int64_t)c * w;
-  for (int i1 = k; i1 > 0;) {
-    const int i0 = i1 > 32 ? i1 - 32 : 0, bs = i1 - i0;
-    double x[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) x[j] = j < bs ? yc[i0 + j] : 0.0;
-#pragma unroll
-    for (int j = 31; j >= 0; --j) {
-      if (j < bs) {
-        double vv = x[j];
-#pragma unroll
-        for (int l = j + 1; l < 32; ++l)
-          if (l < bs) vv -= y(i0 + j, i0 + l) * x[l];
-        x[j] = vv / y(i0 + j, i0 + j);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 32; ++j)
-      if (j < bs) yc[i0 + j] = x[j];
-    for (int rr = 0; rr < i0; ++rr) {
-      double vv = yc[rr];
-      const double* Rr = Y + rr + (int64_t)i0 * w;
-#pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (j < bs) vv -= Rr[(int64_t)j * w] * x[j];
-      yc[rr] = vv;
-    }
-    i1 = i0;
-  }
+  if (k <= 0 || k >= n || k + (int)blockIdx.x * 256 >= n) return;   // uniform over the CTA
+  double* Y = const_cast<double*>(a.ypool) + t.ax_off;
+  tsolve_block_columns(Y, w, k, n, blockIdx.x * 256, n, tsd, tsu);
 }
 
 __global__ void __launch_bounds__(kWThreads) k_gw_out(CompressArgs a, GwState* gs) {

@@ -627,18 +627,8 @@ __device__ __forceinline__ HbOp hb_op(const ElimArgs& a, const ElimTask& t, int 
   return o;
 }
 
-// C tile (64 x 64) -= A B for the box's operation: 4 warps, each 32 x 32 outputs.
-__global__ void __launch_bounds__(128) k_hb_gemm(ElimArgs a, int kind, int j0) {
-  __shared__ double As[kTM * kGld];
-  __shared__ double Bs[kTN * kGld];
-  const ElimTask t = a.tasks[blockIdx.z];
-  const int r = t.n - t.k;
-  if (r <= 0 || j0 >= r) return;
-  if ((kind == HB_TROW || kind == HB_TCOL || kind == HB_EUPD || kind == HB_GUPD || kind == HB_SCHUR) && t.k == 0)
-    return;
-  const HbOp o = hb_op(a, t, kind, j0);
-  const int i0 = blockIdx.x * kTM, c0 = blockIdx.y * kTN;
-  if (i0 >= o.M || c0 >= o.N || o.K <= 0) return;
+// C tile (64 x 64) at (i0, c0) -= A B of the operation: 4 warps, each 32 x 32 outputs.
+__device__ void hb_gemm_tile(const HbOp& o, int i0, int c0, double* As, double* Bs) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tq = lane & 3;
   const int wm = warp >> 1, wn = warp & 1;
@@ -701,6 +691,88 @@ __global__ void __launch_bounds__(128) k_hb_gemm(ElimArgs a, int kind, int j0) {
         const int col = c0 + wn * 32 + j * 8 + 2 * tq + e;
         if (col < o.N) o.C[row * o.crs + col * o.ccs] -= acc[i][j][e];
       }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_hb_gemm(ElimArgs a, int kind, int j0) {
+  __shared__ double As[kTM * kGld];
+  __shared__ double Bs[kTN * kGld];
+  const ElimTask t = a.tasks[blockIdx.z];
+  const int r = t.n - t.k;
+  if (r <= 0 || j0 >= r) return;
+  if ((kind == HB_TROW || kind == HB_TCOL || kind == HB_EUPD || kind == HB_GUPD || kind == HB_SCHUR) && t.k == 0)
+    return;
+  const HbOp o = hb_op(a, t, kind, j0);
+  const int i0 = blockIdx.x * kTM, c0 = blockIdx.y * kTN;
+  if (i0 >= o.M || c0 >= o.N || o.K <= 0) return;
+  hb_gemm_tile(o, i0, c0, As, Bs);
+}
+
+// One explicit product C -= A B over a grid of 64 x 64 tiles (the grid-wide sweep).
+__global__ void __launch_bounds__(128) k_dgemm_op(HbOp o) {
+  __shared__ double As[kTM * kGld];
+  __shared__ double Bs[kTN * kGld];
+  const int i0 = blockIdx.x * kTM, c0 = blockIdx.y * kTN;
+  if (i0 >= o.M || c0 >= o.N || o.K <= 0) return;
+  hb_gemm_tile(o, i0, c0, As, Bs);
+}
+
+// Rows j0..j0+jb of X (r x nrhs, column-major) solved against the diagonal block of the
+// triangular view M (lower: forward, upper: backward; unit diagonal or not), one thread
+// per right-hand side.
+__global__ void __launch_bounds__(256) k_trsm_diag(GV M, double* X, int r, int nrhs, int j0, int jb, int lower,
+                                                   int unit) {
+  __shared__ double blk[kHb * (kHb + 1)];
+  for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
+    const int i = e % jb, c = e / jb;
+    blk[i + c * (kHb + 1)] = M.at(j0 + i, j0 + c);
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= nrhs) return;
+  double* x = X + j0 + (int64_t)col * r;
+  double v[kHb];
+#pragma unroll
+  for (int i = 0; i < kHb; ++i) v[i] = i < jb ? x[i] : 0.0;
+  if (lower) {
+#pragma unroll
+    for (int i = 0; i < kHb; ++i) {
+      if (i < jb) {
+        double s = v[i];
+#pragma unroll
+        for (int l = 0; l < i; ++l) s -= blk[i + l * (kHb + 1)] * v[l];
+        v[i] = unit ? s : s / blk[i + i * (kHb + 1)];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = kHb - 1; i >= 0; --i) {
+      if (i < jb) {
+        double s = v[i];
+#pragma unroll
+        for (int l = i + 1; l < kHb; ++l)
+          if (l < jb) s -= blk[i + l * (kHb + 1)] * v[l];
+        v[i] = unit ? s : s / blk[i + i * (kHb + 1)];
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kHb; ++i)
+    if (i < jb) x[i] = v[i];
+}
+
+// Rows idx[perm ? perm[i] : i] of the point-major work array W (ld nrhs) <-> the dense
+// r x nrhs block X; dir 0 gathers, 1 scatters.
+__global__ void k_rows_gs(double* W, int nrhs, const int64_t* idx, const int32_t* perm, int r, double* X, int dir) {
+  const int64_t total = (int64_t)r * nrhs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e % nrhs);
+    const int i = (int)(e / nrhs);
+    const int64_t pt = idx[perm ? perm[i] : i];
+    if (dir == 0)
+      X[i + (int64_t)c * r] = W[pt * nrhs + c];
+    else
+      W[pt * nrhs + c] = X[i + (int64_t)c * r];
   }
 }
 
@@ -1106,6 +1178,58 @@ void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int 
   if (pslot) cudaFreeAsync(pslot, s);
   const int64_t tot = 4 * (int64_t)std::max(kmax, 1) * rmax + (int64_t)rmax * rmax;
   k_hb_store<<<dim3((unsigned)std::min<int64_t>((tot + kThreads - 1) / kThreads, 4096), 1, z), kThreads, 0, s>>>(a);
+}
+
+int sweep_root_grid(double* W, int nrhs, const int64_t* rd, const int32_t* perm, const double* LU, int r, int op,
+                    int trans, int symm, double* X, cudaStream_t s) {
+  // k = 0: only the triangular factors act (rskelf_sv_*.m with empty sk)
+  const bool lu = symm != 'p';
+  const bool gather_p = lu && op == 0 && trans == 0;
+  const bool scatter_p = lu && op == 1 && trans == 1;
+  GV M;
+  bool lower, unit;
+  if (op == 0) {          // forward: L \ x ('n', or chol), U' \ x ('t')
+    M = (lu && trans) ? GV{LU, (int64_t)r, 1} : GV{LU, 1, (int64_t)r};
+    lower = true;
+    unit = lu && !trans;
+  } else {                // backward: U \ x ('n'), L' \ x (chol, or 't' unit)
+    M = (lu && !trans) ? GV{LU, 1, (int64_t)r} : GV{LU, (int64_t)r, 1};
+    lower = false;
+    unit = lu && trans;
+  }
+  int launches = 0;
+  const unsigned gblk = (unsigned)std::min<int64_t>(((int64_t)r * nrhs + 255) / 256, 148 * 8);
+  k_rows_gs<<<gblk, 256, 0, s>>>(W, nrhs, rd, gather_p ? perm : nullptr, r, X, 0);
+  ++launches;
+  const unsigned cb = (unsigned)((nrhs + 255) / 256);
+  auto tiles = [](int x) { return (unsigned)std::max(1, (x + 63) / 64); };
+  if (lower) {
+    for (int j0 = 0; j0 < r; j0 += kHb) {
+      const int jb = std::min(kHb, r - j0), j1 = j0 + jb;
+      k_trsm_diag<<<cb, 256, 0, s>>>(M, X, r, nrhs, j0, jb, 1, unit ? 1 : 0);
+      ++launches;
+      if (j1 < r) {
+        HbOp o{X + j1, 1, (int64_t)r, GV{M.p + j1 * M.rs + j0 * M.cs, M.rs, M.cs}, GV{X + j0, 1, (int64_t)r},
+               r - j1, nrhs, jb};
+        k_dgemm_op<<<dim3(tiles(r - j1), tiles(nrhs)), 128, 0, s>>>(o);
+        ++launches;
+      }
+    }
+  } else {
+    for (int j1 = r; j1 > 0;) {
+      const int j0 = std::max(0, j1 - kHb), jb = j1 - j0;
+      k_trsm_diag<<<cb, 256, 0, s>>>(M, X, r, nrhs, j0, jb, 0, unit ? 1 : 0);
+      ++launches;
+      if (j0 > 0) {
+        HbOp o{X, 1, (int64_t)r, GV{M.p + j0 * M.cs, M.rs, M.cs}, GV{X + j0, 1, (int64_t)r}, j0, nrhs, jb};
+        k_dgemm_op<<<dim3(tiles(j0), tiles(nrhs)), 128, 0, s>>>(o);
+        ++launches;
+      }
+      j1 = j0;
+    }
+  }
+  k_rows_gs<<<gblk, 256, 0, s>>>(W, nrhs, rd, scatter_p ? perm : nullptr, r, X, 1);
+  return launches + 1;
 }
 
 int elim_huge_launches(int rmax, int kmax, bool chol) {

@@ -81,6 +81,16 @@ void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cuda
 // the largest n, k and r among them.
 void launch_eliminate_huge(const ElimArgs& a, int nbox, int nmax, int kmax, int rmax, cudaStream_t s);
 int elim_huge_launches(int rmax, int kmax, bool chol);
+// The solve sweep (op 0 upward, 1 downward; rskelf_sv_*.m) of a factor with no skeletons
+// (k = 0: the root) and a large redundant block, spread over the GPU: its rows of the
+// point-major work array W gathered into the dense r x nrhs block X (device scratch),
+// blocked triangular solves with the factor's LU (or L) block -- diagonal blocks one
+// thread per right-hand side, off-diagonal updates as FP64 tensor-path GEMMs -- and
+// scattered back.  Returns the number of launches.
+int sweep_root_grid(double* W, int nrhs, const int64_t* rd, const int32_t* perm, const double* LU, int r, int op,
+                    int trans, int symm, double* X, cudaStream_t s);
+// Factors with no skeletons and at least this many redundant rows take sweep_root_grid.
+constexpr int kRootGridR = 1024;
 // Redundant blocks from this size up take the grid-wide elimination.
 constexpr int kHugeR = 320;
 
