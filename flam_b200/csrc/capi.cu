@@ -1264,10 +1264,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         u.l[c] = c0.l[c];
       }
       sk_of[q] = (int)skt.size();
-      // CTAs of the box: all of it in one when it fits 256 x 256, else 128 columns of K by
-      // up to 512 rows of Y each
-      const bool one = u.n <= kSketchCtaCols && u.w <= kSketchCtaCols;
-      const int cstep = one ? u.n : 128, jstep = one ? u.w : kSketchCtaRows;
+      int cstep, jstep;   // the box's CTAs: column and sketch-row extents
+      sketch_cta_tile(o.sketch == 2, u.n, u.w, &cstep, &jstep);
       for (int c0i = 0; c0i < u.n; c0i += cstep)
         for (int j0i = 0; j0i < u.w; j0i += jstep) {
           SketchTask v2 = u;
@@ -1407,6 +1405,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       sa.symm_n = F.symm == 'n' ? 1 : 0;
       sa.seed = o.sketch_seed;
       sa.status = status.p;
+      sa.fp64 = o.sketch == 2;
       size_t smx = 0;
       for (const SketchTask& u : skt) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
       launch_sketch(sa, (int)skt.size(), smx, s);
@@ -1484,13 +1483,15 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
             u.w = wf;
             u.y_off = y2;
             first2.push_back((int)skt2.size());
-            for (int c0i = 0; c0i < u.n; c0i += 128)
-              for (int j0i = 0; j0i < wf; j0i += kSketchCtaRows) {
+            int cstep, jstep;
+            sketch_cta_tile(o.sketch == 2, u.n, wf, &cstep, &jstep);
+            for (int c0i = 0; c0i < u.n; c0i += cstep)
+              for (int j0i = 0; j0i < wf; j0i += jstep) {
                 SketchTask v2 = u;
                 v2.col0 = c0i;
-                v2.ncol = std::min(128, u.n - c0i);
+                v2.ncol = std::min(cstep, u.n - c0i);
                 v2.j0 = j0i;
-                v2.nw = std::min(kSketchCtaRows, wf - j0i);
+                v2.nw = std::min(jstep, wf - j0i);
                 skt2.push_back(v2);
               }
             CompressTask v = ct[q];
@@ -1517,6 +1518,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           sa.symm_n = F.symm == 'n' ? 1 : 0;
           sa.seed = o.sketch_seed ^ 0x9E3779B9u;
           sa.status = status.p;
+          sa.fp64 = o.sketch == 2;
           size_t smx = 0;
           for (const SketchTask& u : skt2) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
           launch_sketch(sa, (int)skt2.size(), smx, s);
@@ -1885,6 +1887,8 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
   if (!(rank_or_tol >= 0)) fail(FLAM_ERR_ARG, "FLAM:id:invalidRankOrTol: Rank or tolerance must be nonnegative.");
   if (!(o.Tmax >= 1)) fail(FLAM_ERR_ARG, "FLAM:id:invalidTmax: Interpolation matrix entry bound must be >= 1.");
   const char symm = chksymm(o.symm);
+  if (o.sketch < 0 || o.sketch > 2)
+    fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidSketch: opts.sketch must be 0 (exact ID), 1 (TF32 sketch) or 2 (FP64 sketch)");
   if (symm == 'h')
     fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h' (LDL) is not available on the device path");
   flam_proxy px{};

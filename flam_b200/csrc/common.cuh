@@ -185,6 +185,26 @@ __device__ __forceinline__ double aentry(const Problem& P, const InstParams& ip,
   return v;
 }
 
+// Row `type` of a box's compression block K at column point sc (rskelf.m:201-212):
+// 0 A(q, sc) for a neighbour q, 1 A(sc, q)' (the transposed block of symm 'n'),
+// 2 the proxy row at point y (multiplier wmul, or the column's weight when 0), 3 zero.
+__device__ __forceinline__ double block_entry(const Problem& P, const InstParams& ip, int type, int64_t q,
+                                              const double* y, double wmul, int64_t sc) {
+  switch (type) {
+    case 0:
+      return aentry(P, ip, q, sc);
+    case 1:
+      return aentry(P, ip, sc, q);
+    case 2: {
+      const double v = ip.pscale * keval(ip.pkernel, ip.pparam, P.d, y, P.x + sc * P.d, nullptr);
+      if (wmul != 0.0) return v * wmul;
+      return ip.has_w ? v * P.w[sc] : v;
+    }
+    default:
+      return 0.0;
+  }
+}
+
 #endif  // __CUDACC__
 
 }  // namespace flam

@@ -80,23 +80,6 @@ __device__ __forceinline__ void reflect_col(double (&p)[B], double al, double* R
   if (g == 0) *tau_out = tau;
 }
 
-__device__ __forceinline__ double entry_of(const Problem& P, const InstParams& ip, int type, int64_t q,
-                                           const double* y, double wmul, int64_t sc) {
-  switch (type) {
-    case 0:
-      return aentry(P, ip, q, sc);
-    case 1:
-      return aentry(P, ip, sc, q);
-    case 2: {
-      const double v = ip.pscale * keval(ip.pkernel, ip.pparam, P.d, y, P.x + sc * P.d, nullptr);
-      if (wmul != 0.0) return v * wmul;
-      return ip.has_w ? v * P.w[sc] : v;
-    }
-    default:
-      return 0.0;
-  }
-}
-
 // pxyfun's neighbour selection (the reference test drivers' filters): stable
 // compaction of the box's candidate list in place; returns the kept count.
 __device__ __forceinline__ int filter_candidates(const CompressTask& t, const Problem& P, const InstParams& ip,
@@ -259,7 +242,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
 #pragma unroll
         for (int i = 0; i < B; ++i) {
           const int s = g * B + i;
-          p[i] = entry_of(P, ip, st.type[s], st.q[s], st.y[s], st.wmul[s], sc);
+          p[i] = block_entry(P, ip, st.type[s], st.q[s], st.y[s], st.wmul[s], sc);
         }
       }
     }

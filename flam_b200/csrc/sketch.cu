@@ -357,6 +357,129 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(SketchArgs a) {
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
+// FP64 form of the sketch (opts.sketch = 2): the same Y = Omega K, with K's entries
+// evaluated in FP64 exactly as the exact compression generates them (block_entry) and the
+// products on the FP64 tensor path (mma.sync m8n8k4 .f64), accumulated in FP64.  The
+// sketch then carries full precision, so the randomized ID meets tight tolerances directly
+// (no refinement needed).  One CTA forms a tile of at most kSketchF64Rows rows of Y by
+// kSketchF64Cols columns of K; chunks of kFk rows of K are staged through shared memory
+// (K transposed, Omega row-major; stride kFld = 20 doubles keeps the fragment loads at two
+// wavefronts), eight warps each own a 32 x 32 block of the tile.
+constexpr int kFk = 16;
+constexpr int kFld = kFk + 4;
+
+__device__ __forceinline__ void dmma_f64(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kSkThreads) k_sketch_f64(SketchArgs a) {
+  __shared__ double Ks[kSketchF64Cols * kFld];
+  __shared__ double Os[kSketchF64Rows * kFld];
+  __shared__ RowDescF rows[kFk];
+  const SketchTask t = a.tasks[blockIdx.x];
+  const Problem& P = a.P;
+  const InstParams ip = P.ip[t.inst];
+  const int n = t.ncol, w = t.nw, d = P.d;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wj = warp >> 2, wc = warp & 3;
+  const int m1 = a.mfilt[t.out_idx];
+  const int nrep = a.symm_n ? 2 : 1;
+  const int npr = (t.flags & 1) ? (ip.two_sided ? 2 * P.npxy : P.npxy) : 0;
+  const int m = nrep * m1 + npr;
+  if (tid == 0) a.mrows[t.out_idx] = m;
+  const int64_t* cand = a.cpool + t.cand_off;
+  // entry (rho, columns cg * 8 .. + 7) of each chunk for this thread
+  const int rho_t = tid & (kFk - 1), cg = tid / kFk;
+  int64_t scol[kSketchF64Cols / (kSkThreads / kFk)];
+#pragma unroll
+  for (int i = 0; i < kSketchF64Cols / (kSkThreads / kFk); ++i) {
+    const int c = cg * (kSketchF64Cols / (kSkThreads / kFk)) + i;
+    scol[i] = c < n ? a.ipool[t.slf_off + t.col0 + c] : -1;
+  }
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int r0 = 0; r0 < m; r0 += kFk) {
+    if (tid < kFk) {
+      const int rho = r0 + tid;
+      RowDescF rd;
+      rd.type = 3;
+      rd.q = -1;
+      rd.wmul = 0.0;
+      rd.y[0] = rd.y[1] = rd.y[2] = 0.0;
+      if (rho < m1) {
+        rd.type = 0;
+        rd.q = cand[rho];
+      } else if (a.symm_n && rho < 2 * m1) {
+        rd.type = 1;
+        rd.q = cand[rho - m1];
+      } else if (rho < m) {
+        int pr = rho - nrep * m1;
+        rd.type = 2;
+        if (ip.two_sided && pr >= P.npxy) {
+          pr -= P.npxy;
+          rd.wmul = ip.wbar;
+        }
+        for (int k = 0; k < d; ++k) {
+          const double pk = P.pxy_pts[pr * d + k];
+          rd.y[k] = P.pxy_shift ? pk + P.pxy_shift[pr * d + k] * t.l[k] + t.ctr[k] : pk * t.l[k] + t.ctr[k];
+        }
+      }
+      rows[tid] = rd;
+    }
+    __syncthreads();   // rows ready; the previous chunk's products are done with Ks / Os
+    {
+      const RowDescF& rd = rows[rho_t];
+#pragma unroll
+      for (int i = 0; i < kSketchF64Cols / (kSkThreads / kFk); ++i) {
+        const int c = cg * (kSketchF64Cols / (kSkThreads / kFk)) + i;
+        Ks[c * kFld + rho_t] =
+            scol[i] >= 0 && rd.type != 3 ? block_entry(P, ip, rd.type, rd.q, rd.y, rd.wmul, scol[i]) : 0.0;
+      }
+    }
+    for (int e = tid; e < kSketchF64Rows * kFk; e += kSkThreads) {
+      const int j = e / kFk, rr = e % kFk, rho = r0 + rr;
+      Os[j * kFld + rr] = (j < w && rho < m) ? (double)omega(a.seed, t.box, rho, t.j0 + j) : 0.0;
+    }
+    __syncthreads();
+    if (wj * 32 < w) {
+      const double* Aw = Os + (wj * 32 + g) * kFld + tq;
+      const double* Bw = Ks + (wc * 32 + g) * kFld + tq;
+#pragma unroll
+      for (int kk = 0; kk < kFk; kk += 4) {
+        double af[4], bf[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] = Aw[i * 8 * kFld + kk];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bf[j] = Bw[j * 8 * kFld + kk];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma_f64(acc[i][j], af[i], bf[j]);
+      }
+    }
+    __syncthreads();
+  }
+  double* Y = a.ypool + t.y_off;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int j = wj * 32 + i * 8 + g;
+    if (j >= w) continue;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = wc * 32 + jj * 8 + 2 * tq + e;
+        if (c < n) Y[(t.j0 + j) + (int64_t)(t.col0 + c) * t.w] = acc[i][jj][e];
+      }
+  }
+}
+
 // Restore the pull-up order of the slf lists of boxes whose sketch was rejected, so the
 // exact compression that redoes them starts from the order the elimination expects.
 __global__ void k_unpermute(const int32_t* idx, const SketchTask* tasks, int64_t* ipool, const int32_t* permpool) {
@@ -378,6 +501,10 @@ size_t sketch_smem_bytes(int ncol, int nw) {
 
 void launch_sketch(const SketchArgs& a, int ntask, size_t smem, cudaStream_t s) {
   if (ntask <= 0) return;
+  if (a.fp64) {
+    k_sketch_f64<<<ntask, kSkThreads, 0, s>>>(a);
+    return;
+  }
   if (ensure_smem_attr(reinterpret_cast<const void*>(k_sketch), (int)smem) != cudaSuccess) return;
   k_sketch<<<ntask, kSkThreads, smem, s>>>(a);
 }

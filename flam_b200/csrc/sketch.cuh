@@ -12,6 +12,22 @@ constexpr int kSketchMaxW = 2048;
 // columns of 128 lanes, i.e. tiles x padded rows <= 512).
 constexpr int kSketchCtaCols = 256;
 constexpr int kSketchCtaRows = 512;
+// The FP64 sketch: one CTA forms at most this many rows of Y by columns of K.
+constexpr int kSketchF64Rows = 64;
+constexpr int kSketchF64Cols = 128;
+
+// Columns of K (cstep) and rows of Y (jstep) one CTA of the sketch of an n-column box
+// with w sketch rows takes.
+inline void sketch_cta_tile(bool fp64, int n, int w, int* cstep, int* jstep) {
+  if (fp64) {
+    *cstep = kSketchF64Cols;
+    *jstep = kSketchF64Rows;
+    return;
+  }
+  const bool one = n <= kSketchCtaCols && w <= kSketchCtaCols;   // the whole box in one CTA
+  *cstep = one ? n : 128;
+  *jstep = one ? w : kSketchCtaRows;
+}
 
 // One box of a factorization step in the sketched form.
 struct SketchTask {
@@ -40,6 +56,7 @@ struct SketchArgs {
   int symm_n;
   uint32_t seed;
   int32_t* status;        // OR of StatusBits (ST_TIMEOUT)
+  int fp64;               // 1: FP64 entries and products (k_sketch_f64), 0: TF32 tensor cores
 };
 
 size_t sketch_smem_bytes(int ncol, int nw);

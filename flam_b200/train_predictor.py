@@ -8,7 +8,7 @@ as a fraction of its point count.  The geometries cycle through the survey's pro
 families at sizes whose factorizations take a fraction of a second -- Matern-3/2 GP
 covariance on uniform points in the unit cube (the learned-rank configuration), the
 3D Laplace second-kind operator on a randomly rotated Fibonacci sphere, and the 2D
-log kernel on seeded star curves -- each at a tolerance drawn from {1e-5, 1e-6, 1e-8}.
+log kernel on seeded star curves -- each at a tolerance drawn from {1e-5, 1e-6, 1e-8, 1e-10}.
 The network is trained on the GPU by the library's own kernels (flam_predictor_train)
 and checked on 10% of the geometries held out.
 """
@@ -27,7 +27,7 @@ def geometry(i):
     """Problem i of the training set: (x, A, pxy, symm, tol)."""
     from . import problems
     rng = np.random.default_rng(1000 + i)
-    tol = float(rng.choice([1e-5, 1e-6, 1e-8]))
+    tol = float(rng.choice([1e-5, 1e-6, 1e-8, 1e-10]))
     fam = i % 3
     if fam == 0:
         N = int(rng.integers(2000, 6000))

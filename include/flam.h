@@ -108,7 +108,9 @@ typedef struct {
    * with the FP64 pivoted QR, rank and R11 \ R12 on Y; boxes of more than 256 points use
    * the exact ID.  A box whose rank comes within sketch_guard of w is redone exactly
    * (the posterior check).  Meant for loose tolerances (>= ~1e-7: the sketch carries
-   * ~21 bits) followed by flam_rskelf_ir_sv. */
+   * ~21 bits) followed by flam_rskelf_ir_sv.  2: the same sketched ID with K's entries and
+   * the products in FP64 (FP64 tensor path), for tight tolerances without refinement.
+   * Other values: FLAM_ERR_ARG (FLAM:rskelf:invalidSketch). */
   int sketch;
   int sketch_p;          /* sketch rows beyond the rank estimate (default 8; w >= 8) */
   int sketch_guard;      /* posterior check margin in rows (default 2) */

@@ -182,3 +182,50 @@ def test_two_host_threads_factor_on_one_device():
     assert not errs, errs
     for a, b in zip(out, ref):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", ["star", "sphere", "matern"])
+def test_fp64_sketch_meets_tight_tolerance_without_refinement(case):
+    """opts.sketch = 2: K's entries and the products in FP64 (FP64 tensor path), so the ID
+    of the sketch meets tol 1e-10 directly; ranks within a few of the exact ID's."""
+    if case == "star":
+        (x, A, pxy), (xo, Ao, po), symm = problems.star(6000, seed=7), configs.star(6000, seed=7), "n"
+    elif case == "sphere":
+        (x, A, pxy), (xo, Ao, po), symm = (problems.sphere(5000, p=128, seed=3), configs.sphere(5000, p=128, seed=3),
+                                           "n")
+    else:
+        (x, A, pxy), (xo, Ao, po), symm = (problems.matern_cube(4000, seed=4, p=32, p_rad=4),
+                                           configs.matern_cube(4000, seed=4, p=32, p_rad=4), "p")
+    tol = 1e-10
+    Fe = fb.rskelf(A, x, 64, tol, pxy, dict(symm=symm))
+    Fs = fb.rskelf(A, x, 64, tol, pxy, dict(symm=symm, sketch=2, profile=True))
+    prof = Fs.profile()
+    assert prof["n_sketch"] > 0
+    assert prof["sketch_rows"] < prof["sketch_rows_k"]
+    ke, _ = _ranks(Fe)
+    ks, _ = _ranks(Fs)
+    assert Fe.info()["nstep"] == Fs.info()["nstep"]
+    assert abs(int(ks.sum()) - int(ke.sum())) <= 0.05 * ke.sum() + 5
+    N = x.shape[1]
+    D = Ao.dense()
+    B = np.asfortranarray(np.random.default_rng(2).standard_normal((N, 3)))
+    for F in (Fe, Fs):
+        X = fb.rskelf_sv(F, B)
+        r = np.linalg.norm(D @ X - B, axis=0) / np.linalg.norm(B, axis=0)
+        assert r.max() <= 1e-10, r
+
+
+def test_fp64_sketch_with_predicted_widths_and_invalid_option():
+    x, A, pxy = problems.star(12000, seed=8)
+    xo, Ao, po = configs.star(12000, seed=8)
+    import os
+    pred = fb.Predictor.load(os.path.join(os.path.dirname(fb.__file__), "predictor_weights.npz"))
+    F = fb.rskelf(A, x, 64, 1e-10, pxy, dict(symm="n", sketch=2, predictor=pred, profile=True))
+    prof = F.profile()
+    assert prof["n_sketch"] > 0
+    B = np.asfortranarray(np.random.default_rng(3).standard_normal((12000, 2)))
+    X = fb.rskelf_sv(F, B)
+    D = Ao.dense()
+    assert (np.linalg.norm(D @ X - B, axis=0) / np.linalg.norm(B, axis=0)).max() <= 1e-10
+    with pytest.raises(fb.FlamError, match="invalidSketch"):
+        fb.rskelf(A, x, 64, 1e-10, pxy, dict(symm="n", sketch=3))
