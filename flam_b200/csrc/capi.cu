@@ -217,7 +217,7 @@ struct Workspace {
   // sketched compression: row sketches, their tasks, rows of K per box, boxes redone exactly
   DBuf<double> ypool;
   DBuf<SketchTask> sktask;
-  DBuf<CompressTask> skfilt, redo_task, wtask;
+  DBuf<CompressTask> skfilt, redo_task, wtask, rsk_task;
   DBuf<int32_t> mrows, redo_idx;
   DBuf<CompressTask> ftask;
   DBuf<unsigned char> gwstate;
@@ -1223,14 +1223,15 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     // pivot step over the GPU, many take one CTA each
     auto launch_wide = [&](const CompressArgs& cw, const std::vector<CompressTask>& tasks) {
       const int nt = (int)tasks.size();
-      if (nt < 148) {
-        int nmx = 0, steps = 0;
-        for (const CompressTask& u : tasks) {
-          nmx = std::max(nmx, u.n);
-          steps = std::max(steps, std::min(u.n, u.ax_rows));
-        }
+      int nmx = 0, wmx = 0, steps = 0;
+      for (const CompressTask& u : tasks) {
+        nmx = std::max(nmx, u.n);
+        wmx = std::max(wmx, u.ax_rows);
+        steps = std::max(steps, std::min(u.n, u.ax_rows));
+      }
+      if (nt < 148 || wmx > cpqr_wide_max_rows()) {
         ws.gwstate.ensure((int64_t)cpqr_grid_state_bytes(nt), s);
-        launch_cpqr_grid(cw, nt, nmx, steps, ws.gwstate.p, s);
+        launch_cpqr_grid(cw, nt, nmx, wmx, steps, ws.gwstate.p, s);
         F.prof.launches += 5 + 2 * steps;
       } else {
         launch_cpqr_wide(cw, nt, s);
@@ -1459,22 +1460,21 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           launch_unpermute(ws.redo_idx.p, (int)ridx.size(), ws.sktask.p, F.ipool.p, permpool.p, nmx, s);
           F.prof.launches += 1;
         }
-        // boxes wider than the thread-per-column compression get a second sketch at full
-        // width n + p (the rank cannot fill it unless the width is capped); the others, and
-        // any box whose second sketch fills too, take the exact ID
+        // a second sketch at full width n + p (the rank cannot fill it); a box whose first
+        // sketch already had that width, or whose second sketch fills too, takes the exact ID
         std::vector<int> exact;
         std::vector<int> resk;
         const int spf = std::max(o.sketch_p, 8);
         for (int q : redo) {
           const int wf = std::min((int)nslf[q] + spf, kSketchMaxW);
-          if (nslf[q] > kTcMaxN && wf > skw[q])
+          if (wf > skw[q])
             resk.push_back(q);
           else
             exact.push_back(q);
         }
         if (!resk.empty()) {
           std::vector<SketchTask> skt2;
-          std::vector<CompressTask> wts2;
+          std::vector<CompressTask> wts2, nts2;   // IDs of the second sketches: wide, thread-per-column
           std::vector<int> first2;
           int64_t y2 = 0;
           for (int q : resk) {
@@ -1500,7 +1500,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
             v.ax_off = y2;
             v.ax_rows = wf;
             v.ax_guard = sk_guard;
-            wts2.push_back(v);
+            (v.n > kTcMaxN ? wts2 : nts2).push_back(v);
             F.prof.id_rows += skw[q];   // the first sketch's rows
             skw[q] = wf;
             y2 += (int64_t)wf * nslf[q];
@@ -1522,12 +1522,35 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           size_t smx = 0;
           for (const SketchTask& u : skt2) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
           launch_sketch(sa, (int)skt2.size(), smx, s);
-          ws.wtask.upload(wts2, s);
-          CompressArgs cw = ca;
-          cw.tasks = ws.wtask.p;
-          cw.ypool = ws.ypool.p;
-          launch_wide(cw, wts2);
           F.prof.launches += 1;
+          if (!wts2.empty()) {
+            ws.wtask.upload(wts2, s);
+            CompressArgs cw = ca;
+            cw.tasks = ws.wtask.p;
+            cw.ypool = ws.ypool.p;
+            launch_wide(cw, wts2);
+          }
+          if (!nts2.empty()) {   // grouped by kernel shape, as the first pass
+            std::stable_sort(nts2.begin(), nts2.end(), [&](const CompressTask& x, const CompressTask& y) {
+              return kkey_n(x.n) < kkey_n(y.n);
+            });
+            ws.rsk_task.upload(nts2, s);
+            for (size_t b0 = 0; b0 < nts2.size();) {
+              const int key = kkey_n(nts2[b0].n);
+              size_t b1 = b0;
+              size_t sm = 16;
+              while (b1 < nts2.size() && kkey_n(nts2[b1].n) == key) {
+                if (nts2[b1].scr_off < 0) sm = std::max(sm, compress_tc_smem_bytes(nts2[b1].n));
+                ++b1;
+              }
+              CompressArgs cr = ca;
+              cr.tasks = ws.rsk_task.p + b0;
+              cr.ypool = ws.ypool.p;
+              launch_compress_tc(cr, (int)(b1 - b0), key / 1000, (key / 10) % 100, key % 10, sm, s);
+              F.prof.launches += 1;
+              b0 = b1;
+            }
+          }
           CK(cudaGetLastError());
           auto co3 = download(cout.p, nb, s);
           std::vector<int32_t> ridx2;

@@ -15,13 +15,15 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "rrqr.cuh"
+#include "sketch.cuh"
 
 namespace flam {
 namespace {
 
 constexpr int kWThreads = 512;
 constexpr int kWWarps = kWThreads / 32;
-constexpr int kWMaxRows = 2048;
+constexpr int kWMaxRows = 2048;          // single-CTA form (its reflector lives in shared memory)
+constexpr int kGwMaxRows = kSketchMaxW;   // grid form (reflector in dynamic shared memory)
 
 struct WAm {
   double v;
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_norms(CompressArgs a, GwState*
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     GwState z{};
-    z.stop = (n == 0 || w > kWMaxRows) ? 0 : min(w, n);
+    z.stop = (n == 0 || w > kGwMaxRows) ? 0 : min(w, n);
     z.r00 = 0.0;
     gs[blockIdx.y] = z;
   }
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_pivot(CompressArgs a, GwState*
 }
 
 __global__ void __launch_bounds__(kWThreads) k_gw_apply(CompressArgs a, GwState* gs, int i) {
-  __shared__ double v[kWMaxRows];
+  extern __shared__ double v[];   // rows of the reflector (w doubles)
   const int b = blockIdx.y;
   if (i >= gs[b].stop) return;
   const CompressTask t = a.tasks[b];
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_rank(CompressArgs a, GwState* 
     int kmax = a.kmax;
     if (kmax == 0 || kmax > n) kmax = n;
     gs[b].ktol = kt;
-    gs[b].k = (n == 0 || w > kWMaxRows) ? 0 : min(kt, kmax);
+    gs[b].k = (n == 0 || w > kGwMaxRows) ? 0 : min(kt, kmax);
     s_ktol = kt;
   }
   __syncthreads();
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_out(CompressArgs a, GwState* g
   const int n = t.n, w = t.ax_rows;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   CompressOut* out = a.out + t.out_idx;
-  if (n == 0 || w > kWMaxRows) {
+  if (n == 0 || w > kGwMaxRows) {
     if (tid == 0) *out = CompressOut{0, 0, 0, n == 0 ? 0 : (int)ST_ID_CHECK};
     return;
   }
@@ -561,14 +563,18 @@ void launch_cpqr_wide(const CompressArgs& a, int ntask, cudaStream_t s) {
 
 size_t cpqr_grid_state_bytes(int ntask) { return sizeof(GwState) * (size_t)std::max(ntask, 1); }
 
-void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int steps, void* state, cudaStream_t s) {
+int cpqr_wide_max_rows() { return kWMaxRows; }
+
+void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int wmax, int steps, void* state, cudaStream_t s) {
   if (ntask <= 0) return;
   GwState* gs = static_cast<GwState*>(state);
   const unsigned cb = (unsigned)((nmax + kWWarps - 1) / kWWarps), z = (unsigned)ntask;
+  const int vbytes = (int)sizeof(double) * std::max(1, std::min(wmax, kGwMaxRows));
+  if (ensure_smem_attr(reinterpret_cast<const void*>(k_gw_apply), vbytes) != cudaSuccess) return;
   k_gw_norms<<<dim3(cb, z), kWThreads, 0, s>>>(a, gs);
   for (int i = 0; i < steps; ++i) {
     k_gw_pivot<<<z, kWThreads, 0, s>>>(a, gs, i);
-    k_gw_apply<<<dim3(cb, z), kWThreads, 0, s>>>(a, gs, i);
+    k_gw_apply<<<dim3(cb, z), kWThreads, vbytes, s>>>(a, gs, i);
   }
   k_gw_rank<<<z, kWThreads, 0, s>>>(a, gs);
   k_gw_tsolve<<<dim3((unsigned)((nmax + 255) / 256), z), 256, 0, s>>>(a, gs);

@@ -49,7 +49,10 @@ void launch_cpqr_wide(const CompressArgs& a, int ntask, cudaStream_t s);
 // for `steps` steps (>= min(rows, n) of every task), per-task state of
 // cpqr_grid_state_bytes(ntask) bytes in device memory.
 size_t cpqr_grid_state_bytes(int ntask);
-void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int steps, void* state, cudaStream_t s);
+// wmax: the most sketch rows of a task (at most kSketchMaxW).
+void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int wmax, int steps, void* state, cudaStream_t s);
+// Sketch rows the single-CTA form (launch_cpqr_wide) takes at most.
+int cpqr_wide_max_rows();
 // Neighbour filter alone (row-split form): tasks[0, ntask) compact their candidates
 // and write the kept count to a.mfilt[out_idx].
 void launch_filter(const CompressArgs& a, int ntask, cudaStream_t s);

@@ -7,7 +7,9 @@ namespace flam {
 // Boxes up to this many points are sketched (two 128-column tiles of tensor memory);
 // larger boxes take the exact compression.
 constexpr int kSketchMaxN = 8192;
-constexpr int kSketchMaxW = 2048;
+// Sketch rows at most: a box's full width plus the oversampling, so that a second sketch
+// can always hold the rank.
+constexpr int kSketchMaxW = kSketchMaxN + 64;
 // One CTA sketches at most this many columns of K and rows of Y (tensor memory: 512 FP32
 // columns of 128 lanes, i.e. tiles x padded rows <= 512).
 constexpr int kSketchCtaCols = 256;
