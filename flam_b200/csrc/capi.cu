@@ -987,6 +987,20 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     cudaEvent_t e0, e1;
   };
   std::vector<LaunchRec> lrec;
+  // FLAM_PROFILE=2: event pairs around the phases of the sketched compression on stream s
+  // (key -1 filter + sketch, -2 ID of the wide sketches, -3 second sketch, -4 ID of the wide
+  // second sketches, -5 ID of the narrow second sketches, -6 exact redo)
+  auto ph_begin = [&](int key, cudaStream_t st) {
+    if (!(prof && prof_launch)) return;
+    LaunchRec lr{key, 0, 0, nullptr, nullptr};
+    CK(cudaEventCreate(&lr.e0));
+    CK(cudaEventCreate(&lr.e1));
+    CK(cudaEventRecord(lr.e0, st));
+    lrec.push_back(lr);
+  };
+  auto ph_end = [&](cudaStream_t st) {
+    if (prof && prof_launch) CK(cudaEventRecord(lrec.back().e1, st));
+  };
   // per-step CUDA events around the compress and elimination launches; resolved
   // after the last step so that profiling adds no synchronisation
   std::vector<cudaEvent_t> step_ev;
@@ -1331,6 +1345,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ca.scratch = scratch.p;
     ca.out = cout.p;
     ca.rel_tol = rel_tol;
+    ca.sketch_rel_tol = rel_tol * kSketchTolScale;
     ca.kmax = kmax;
     ca.symm_n = F.symm == 'n' ? 1 : 0;
     ca.Tmax = o.Tmax;
@@ -1389,6 +1404,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       if (nuse > 1) ws.join_to(s, nuse);
     };
     if (!skt.empty()) {   // neighbour filter and row sketch of the sketched boxes, before their IDs
+      ph_begin(-1, s);
       ws.mrows.ensure(nb, s);
       ws.sktask.upload(skt, s);
       ws.skfilt.upload(skf, s);
@@ -1410,12 +1426,15 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       size_t smx = 0;
       for (const SketchTask& u : skt) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
       launch_sketch(sa, (int)skt.size(), smx, s);
+      ph_end(s);
       F.prof.launches += 2;
       if (!wts.empty()) {
+        ph_begin(-2, s);
         ws.wtask.upload(wts, s);
         CompressArgs cw = ca;
         cw.tasks = ws.wtask.p;
         launch_wide(cw, wts);
+        ph_end(s);
       }
       F.prof.n_sketch += (int64_t)skf.size();
     }
@@ -1521,16 +1540,21 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           sa.fp64 = o.sketch == 2;
           size_t smx = 0;
           for (const SketchTask& u : skt2) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
+          ph_begin(-3, s);
           launch_sketch(sa, (int)skt2.size(), smx, s);
+          ph_end(s);
           F.prof.launches += 1;
           if (!wts2.empty()) {
+            ph_begin(-4, s);
             ws.wtask.upload(wts2, s);
             CompressArgs cw = ca;
             cw.tasks = ws.wtask.p;
             cw.ypool = ws.ypool.p;
             launch_wide(cw, wts2);
+            ph_end(s);
           }
           if (!nts2.empty()) {   // grouped by kernel shape, as the first pass
+            ph_begin(-5, s);
             std::stable_sort(nts2.begin(), nts2.end(), [&](const CompressTask& x, const CompressTask& y) {
               return kkey_n(x.n) < kkey_n(y.n);
             });
@@ -1550,6 +1574,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
               F.prof.launches += 1;
               b0 = b1;
             }
+            ph_end(s);
           }
           CK(cudaGetLastError());
           auto co3 = download(cout.p, nb, s);
@@ -1581,6 +1606,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         std::stable_sort(rt.begin(), rt.end(),
                          [&](const CompressTask& x, const CompressTask& y) { return kkey_n(x.n) < kkey_n(y.n); });
         ws.redo_task.upload(rt, s);
+        if (!rt.empty()) ph_begin(-6, s);
         for (size_t b0 = 0; b0 < rt.size();) {
           const int key = kkey_n(rt[b0].n);
           size_t b1 = b0;
@@ -1598,6 +1624,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           F.prof.launches += 1;
           b0 = b1;
         }
+        if (!rt.empty()) ph_end(s);
         CK(cudaGetLastError());
         F.prof.n_sketch_redo += (int64_t)redo.size();
         auto co2 = download(cout.p, nb, s);
@@ -1770,9 +1797,14 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
         nit += co[q].niter;
         nbig += nslf[q] > kSmemN;
       }
+      int wmx = 0, nsk = 0;
+      for (int q = 0; q < nb; ++q) {
+        wmx = std::max(wmx, skw[q]);
+        nsk += skw[q] > 0;
+      }
       fprintf(stderr, "[flam] step %2d boxes %6d nmax %5lld big %4lld candmax %6lld mmax %6lld kmax %4lld rrqr %5lld"
-              "  compress %8.3f ms  elim %8.3f ms\n", step, nb, (long long)nmx, (long long)nbig, (long long)cmx,
-              (long long)mmx, (long long)kmx2, (long long)nit, tc, tel);
+              "  compress %8.3f ms  elim %8.3f ms  sketched %d wmax %d\n", step, nb, (long long)nmx, (long long)nbig,
+              (long long)cmx, (long long)mmx, (long long)kmx2, (long long)nit, tc, tel, nsk, wmx);
       // per launch: tasks, sum of n, reflector steps of the row folding (panels x n)
       for (LaunchRec& lr : lrec) {
         float tl = 0;
@@ -2700,6 +2732,7 @@ flam_status flam_id(const double* A, int64_t m, int64_t n, int64_t lda, double r
     ca.scratch = scr.p;
     ca.out = co.p;
     ca.rel_tol = std::fmod(rank_or_tol, 1.0);
+    ca.sketch_rel_tol = ca.rel_tol * kSketchTolScale;
     ca.kmax = (int)std::min<double>(std::floor(rank_or_tol), 2e9);
     ca.symm_n = 0;
     ca.Tmax = Tmax;

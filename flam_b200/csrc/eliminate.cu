@@ -22,6 +22,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+// Dynamic shared memory of k_eliminate_big's LU panel: with its ~29 KB of static shared
+// memory this stays inside the 227 KB a CTA may hold.
+constexpr int kBigPanBytes = 192 * 1024;
 
 struct AM {
   double v;
@@ -1246,7 +1249,7 @@ int64_t elim_scratch_doubles(int n) { return (int64_t)n * n + (3 * (int64_t)n) /
 
 void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cudaStream_t s) {
   if (ensure_smem_attr(reinterpret_cast<const void*>(k_eliminate), 200 * 1024) != cudaSuccess ||
-      ensure_smem_attr(reinterpret_cast<const void*>(k_eliminate_big), 200 * 1024) != cudaSuccess)
+      ensure_smem_attr(reinterpret_cast<const void*>(k_eliminate_big), kBigPanBytes) != cudaSuccess)
     return;
   if (nsmall > 0) k_eliminate<<<nsmall, kThreads, smem, s>>>(a);
   if (nbig > 0) {
@@ -1257,9 +1260,9 @@ void launch_eliminate(const ElimArgs& a, int nsmall, int nbig, size_t smem, cuda
   }
 }
 
-// Rows of the largest LU panel k_eliminate_big stages in shared memory (200 KB of kNb
+// Rows of the largest LU panel k_eliminate_big stages in shared memory (kBigPanBytes of kNb
 // columns); the kernel holds all 65,536 registers of an SM, so the shared memory costs no
 // occupancy.
-int elim_pan_rows_max() { return (200 * 1024) / (int)(sizeof(double) * kNb); }
+int elim_pan_rows_max() { return kBigPanBytes / (int)(sizeof(double) * kNb); }
 
 }  // namespace flam
