@@ -66,7 +66,8 @@ class FlamProf(C.Structure):
                 ("flop_compress", C.c_double), ("flop_elim", C.c_double), ("flop_sweep", C.c_double),
                 ("byte_sweep", C.c_double), ("n_sketch", C.c_int64), ("n_sketch_redo", C.c_int64),
                 ("sketch_rows", C.c_int64), ("sketch_rows_k", C.c_int64), ("id_rows", C.c_int64),
-                ("graph_replays", C.c_int64)]
+                ("graph_replays", C.c_int64), ("t_sketch", C.c_double), ("flop_sketch", C.c_double),
+                ("flop_id", C.c_double)]
 
 
 class FlamError(RuntimeError):

@@ -122,6 +122,17 @@ std::vector<T> download(const T* p, int64_t n, cudaStream_t s) {
   return v;
 }
 
+// FP64 work of an ID as run on `rows` x n rows (the TSQR fold when rows > n, then k
+// pivoted Householder steps on the n x n R and R11 \ R12).
+double id_flops(double rows, double n, double k) {
+  double f = 0.0;
+  if (rows > n) f += 2 * rows * n * n - 2.0 / 3.0 * n * n * n;
+  const double a = std::min(rows, n);
+  k = std::min(k, a);
+  f += 4 * a * n * k - 2 * (a + n) * k * k + 4.0 / 3.0 * k * k * k;
+  return f + k * k * (n - k);
+}
+
 struct HostFac {
   int inst, step;
   int64_t sk_off;
@@ -1001,6 +1012,18 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   auto ph_end = [&](cudaStream_t st) {
     if (prof && prof_launch) CK(cudaEventRecord(lrec.back().e1, st));
   };
+  // profiling: event pairs around the sketch launches, resolved with the step events
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> sk_ev;
+  auto sk_begin = [&](cudaStream_t st) {
+    if (!prof) return;
+    sk_ev.emplace_back();
+    CK(cudaEventCreate(&sk_ev.back().first));
+    CK(cudaEventCreate(&sk_ev.back().second));
+    CK(cudaEventRecord(sk_ev.back().first, st));
+  };
+  auto sk_end = [&](cudaStream_t st) {
+    if (prof) CK(cudaEventRecord(sk_ev.back().second, st));
+  };
   // per-step CUDA events around the compress and elimination launches; resolved
   // after the last step so that profiling adds no synchronisation
   std::vector<cudaEvent_t> step_ev;
@@ -1345,7 +1368,6 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     ca.scratch = scratch.p;
     ca.out = cout.p;
     ca.rel_tol = rel_tol;
-    ca.sketch_rel_tol = rel_tol * kSketchTolScale;
     ca.kmax = kmax;
     ca.symm_n = F.symm == 'n' ? 1 : 0;
     ca.Tmax = o.Tmax;
@@ -1425,7 +1447,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       sa.fp64 = o.sketch == 2;
       size_t smx = 0;
       for (const SketchTask& u : skt) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
+      sk_begin(s);
       launch_sketch(sa, (int)skt.size(), smx, s);
+      sk_end(s);
       ph_end(s);
       F.prof.launches += 2;
       if (!wts.empty()) {
@@ -1464,6 +1488,7 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           co[q].m = mr[q];   // rows of K, for the work accounting
           F.prof.sketch_rows += skw[q];
           F.prof.sketch_rows_k += mr[q];
+          F.prof.flop_sketch += (o.sketch == 2 ? 2.0 : 4.0) * skw[q] * (double)mr[q] * (double)nslf[q];
         }
       if (!redo.empty()) {
         auto mf = download(ws.mfilt.p, nb, s);
@@ -1521,6 +1546,8 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
             v.ax_guard = sk_guard;
             (v.n > kTcMaxN ? wts2 : nts2).push_back(v);
             F.prof.id_rows += skw[q];   // the first sketch's rows
+            F.prof.flop_id += id_flops(skw[q], nslf[q], co[q].k);
+            F.prof.flop_sketch += (o.sketch == 2 ? 2.0 : 4.0) * wf * (double)mr[q] * (double)nslf[q];
             skw[q] = wf;
             y2 += (int64_t)wf * nslf[q];
           }
@@ -1541,7 +1568,9 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
           size_t smx = 0;
           for (const SketchTask& u : skt2) smx = std::max(smx, sketch_smem_bytes(u.ncol, u.nw));
           ph_begin(-3, s);
+          sk_begin(s);
           launch_sketch(sa, (int)skt2.size(), smx, s);
+          sk_end(s);
           ph_end(s);
           F.prof.launches += 1;
           if (!wts2.empty()) {
@@ -1635,8 +1664,12 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
       }
     }
 
-    for (int q = 0; q < nb; ++q)   // a redone box folded its sketch and then K
+    for (int q = 0; q < nb; ++q) {   // a redone box folded its sketch and then K
       F.prof.id_rows += skw[q] > 0 ? skw[q] + (redone[q] ? co[q].m : 0) : co[q].m;
+      if (nslf[q] > 0)
+        F.prof.flop_id += id_flops(skw[q] > 0 && !redone[q] ? skw[q] : co[q].m, nslf[q], co[q].k) +
+                          (redone[q] ? id_flops(skw[q], nslf[q], co[q].k) : 0.0);
+    }
     if (o.rank_log) {   // features and k/n of every box that was compressed (n > 0)
       auto fv = download(ws.feat.p, (int64_t)nb * kPredFeatures, s);
       for (int q = 0; q < nb; ++q) {
@@ -1903,6 +1936,13 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
   if (prof_print && !step_ev.empty())
     fprintf(stderr, "[flam] gaps: compress->elim %.3f ms  elim->next compress %.3f ms\n", gap_elim, gap_next);
   for (auto& e : step_ev) CK(cudaEventDestroy(e));
+  for (auto& e : sk_ev) {
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e.first, e.second));
+    F.prof.t_sketch += t * 1e-3;
+    CK(cudaEventDestroy(e.first));
+    CK(cudaEventDestroy(e.second));
+  }
   CK(cudaStreamSynchronize(s));
   if (st & ST_NOT_SPD)
     fail(FLAM_ERR_NOT_SPD, "FLAM:rskelf:notPosDef: a redundant block is not positive definite (chol failed)");
@@ -2732,7 +2772,6 @@ flam_status flam_id(const double* A, int64_t m, int64_t n, int64_t lda, double r
     ca.scratch = scr.p;
     ca.out = co.p;
     ca.rel_tol = std::fmod(rank_or_tol, 1.0);
-    ca.sketch_rel_tol = ca.rel_tol * kSketchTolScale;
     ca.kmax = (int)std::min<double>(std::floor(rank_or_tol), 2e9);
     ca.symm_n = 0;
     ca.Tmax = Tmax;

@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     const double al = R[(int64_t)i * ld + i];
     const double dii = s != 0.0 ? -copysign(hypot(al, sqrt(s)), al) : al;   // R(i,i) after this step
     if (i == 0) r00 = fabs(dii);
-    if (stop_early && i > 0 && !(fabs(dii) > (t.ax_rows > 0 ? a.sketch_rel_tol : a.rel_tol) * r00)) {
+    if (stop_early && i > 0 && !(fabs(dii) > a.rel_tol * r00)) {
       mn_eff = i;      // uniform: every thread computed the same dii
       break;
     }
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
 
   // ---- (4) rank (id.m:106-113)
   if (tid == 0) {
-    const double tol = (t.ax_rows > 0 ? a.sketch_rel_tol : a.rel_tol) * fabs(R[0]);
+    const double tol = a.rel_tol * fabs(R[0]);
     int kt = 0;
     if (m > 0)
       for (int i = 0; i < mn_eff; ++i) kt += fabs(R[(int64_t)i * ld + i]) > tol;
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
       __syncthreads();
       if (tid == 0) {
         int niter = 0, capped = 0;
-        const double tol = (t.ax_rows > 0 ? a.sketch_rel_tol : a.rel_tol) * fabs(R[0]);
+        const double tol = a.rel_tol * fabs(R[0]);
         const int kk = rrqr_serial(R, ld, 1, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped, true);
         s_k = kk;
         s_niter = niter;

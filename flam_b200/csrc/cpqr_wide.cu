@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
       const double al = vbuf[i];
       const double dii = ss != 0.0 ? -copysign(hypot(al, sqrt(ss)), al) : al;
       if (i == 0) s_r00 = fabs(dii);
-      if (stop_early && i > 0 && !(fabs(dii) > a.sketch_rel_tol * s_r00)) {
+      if (stop_early && i > 0 && !(fabs(dii) > a.rel_tol * s_r00)) {
         s_stop = i;
         s_tau = -1.0;
       } else {
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
   // rank (id.m:106-113)
   if (tid == 0) {
     const int mn_eff = s_stop;
-    const double tol = a.sketch_rel_tol * fabs(y(0, 0));
+    const double tol = a.rel_tol * fabs(y(0, 0));
     int kt = 0;
     for (int i = 0; i < mn_eff; ++i) kt += fabs(y(i, i)) > tol;
     int kmax = a.kmax;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
       s_need = (ktol > k || bm > a.Tmax * a.Tmax) ? 1 : 0;
       if (s_need) {
         int niter = 0, capped = 0;
-        const double tol = a.sketch_rel_tol * fabs(y(0, 0));
+        const double tol = a.rel_tol * fabs(y(0, 0));
         s_k = rrqr_serial(Y, 1, w, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped);
         s_niter = niter;
         s_cap = capped;
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_pivot(CompressArgs a, GwState*
   const double al = y(i, i);
   const double dii = ss != 0.0 ? -copysign(hypot(al, sqrt(ss)), al) : al;
   const double r00 = i == 0 ? fabs(dii) : gs[b].r00;
-  if (a.kmax == 0 && i > 0 && !(fabs(dii) > a.sketch_rel_tol * r00)) {   // rank reached (tolerance mode)
+  if (a.kmax == 0 && i > 0 && !(fabs(dii) > a.rel_tol * r00)) {   // rank reached (tolerance mode)
     __syncthreads();
     if (tid == 0) gs[b].stop = i;
     return;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_rank(CompressArgs a, GwState* 
   __shared__ int s_ktol;
   if (threadIdx.x == 0) {
     const int mn_eff = gs[b].stop;
-    const double tol = a.sketch_rel_tol * fabs(Y[0]);
+    const double tol = a.rel_tol * fabs(Y[0]);
     int kt = 0;
     for (int i = 0; i < mn_eff; ++i) kt += fabs(Y[i + (int64_t)i * w]) > tol;
     int kmax = a.kmax;
@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_out(CompressArgs a, GwState* g
       for (int q = 0; q < kWWarps; ++q) bm = fmax(bm, red[q]);
       if (ktol > k || bm > a.Tmax * a.Tmax) {
         int niter = 0, capped = 0;
-        const double tol = a.sketch_rel_tol * fabs(y(0, 0));
+        const double tol = a.rel_tol * fabs(y(0, 0));
         s_k = rrqr_serial(Y, 1, w, n, k, ktol, jpvt, tol, a.Tmax, a.rrqr_iter, aux, &niter, &capped);
         gs[b].niter = niter;
         gs[b].cap = capped;

@@ -14,11 +14,6 @@ struct CompressArgs {
   double* scratch;     // work matrices of boxes with n > kSmemN
   CompressOut* out;
   double rel_tol;      // rem(rank_or_tol, 1)
-  // Relative tolerance of the IDs of row sketches (tasks with ax_rows > 0): below rel_tol by
-  // kSketchTolScale, since the interpolation error of a sketched ID exceeds the sketch's own
-  // trailing diagonal by a factor that grows with the rank (about sqrt(k / p) for p rows of
-  // oversampling).
-  double sketch_rel_tol;
   int kmax;            // floor(rank_or_tol)
   int symm_n;          // 1: compress [A(nbr,slf); A(slf,nbr)'; Kpxy] (symm 'n')
   double Tmax;
@@ -28,8 +23,6 @@ struct CompressArgs {
   int32_t* mfilt;      // per box (out_idx): candidates kept by the neighbour filter (row-split form)
   const double* ypool; // row sketches of the sketched boxes (CompressTask::ax_off)
 };
-
-constexpr double kSketchTolScale = 0.1;
 
 size_t compress_smem_bytes(int n);
 int64_t compress_scratch_doubles(int n);

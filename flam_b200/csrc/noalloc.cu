@@ -170,7 +170,6 @@ extern "C" flam_status flam_id_noalloc(const double* A, int64_t m, int64_t n, in
   ca.scratch = reinterpret_cast<double*>(base + kOffDummy);
   ca.out = reinterpret_cast<CompressOut*>(base + kOffOut);
   ca.rel_tol = std::fmod(rank_or_tol, 1.0);
-  ca.sketch_rel_tol = ca.rel_tol * kSketchTolScale;
   ca.kmax = (int)std::min<double>(std::floor(rank_or_tol), 2e9);
   ca.symm_n = 0;
   ca.Tmax = Tmax;

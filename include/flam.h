@@ -400,6 +400,11 @@ typedef struct {
   int64_t sketch_rows_k;   /* sum over the same boxes of rows(K), the rows the exact ID folds */
   int64_t id_rows;         /* rows every ID of the factorization folded (w if sketched, else rows(K)) */
   int64_t graph_replays;   /* applies run as a replayed CUDA graph of their sweep launches */
+  /* executed work of the sketched form (t_compress and flop_compress count the reference's
+   * operations on the full blocks K, which the sketch replaces) */
+  double t_sketch;         /* seconds in the row-sketch launches (part of t_compress) */
+  double flop_sketch;      /* their products: 2 w rows(K) n per sketch (x2 for the TF32 hi/lo split) */
+  double flop_id;          /* pivoted QR + R11 \ R12 as run: on the w sketch rows, else on K */
 } flam_prof;
 
 FLAM_API flam_status flam_profile(const flam_factor* F, flam_prof* out, int reset);
