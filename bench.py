@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""rskelf factor+solve throughput (DOF/s) on B200: plain FP64 and the chosen form.
+"""rskelf factor+solve throughput (DOF/s) on B200 to 1e-10: the chosen form and plain FP64.
 
 Workload (one "step"): build the tree, factor, and solve 256 right-hand sides
 for N = 262144 points on the star curve r(t) = 1 + 0.3 cos 5t with t drawn
@@ -10,25 +10,26 @@ instance (seed = rank), so per-GPU work is fixed as the GPU count grows.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl flam|reference]
 
-value     plain FP64 DOF/s with the inputs resident in HBM (CUDA events on the
-          launch stream, max over ranks).
-e2e       the same through the public API with pinned host buffers, the
-          host<->device copies inside the timed region.
-accuracy  the FP64 relative residual of all 256 solutions, from the library's
-          on-the-fly FP64 matvec (not timed).
-chosen_form (rank 0)  the metric's comparison: the mixed-precision form -- row
-          sketches formed in FP32/TF32 on the tensor cores, sketch widths from the
-          learned rank predictor, FP64 pivots and R11 \\ R12, the factorization at a
-          loose tolerance refined in FP64 to 1e-10 against the FP64 matvec --
-          against plain FP64 at 1e-10, on this workload and on the 3D sphere of the
-          mixed-precision configuration (Fibonacci points with a random rotation,
-          3D Laplace, 256-point proxy sphere, 64 RHS), each with its FP64 error.
+value       DOF/s of the chosen form (flam_b200/chosen.py picks it per problem: here
+            FP64 row sketches on the FP64 tensor path with learned widths, the
+            factorization at 1e-10 and one rskelf_sv) with the inputs resident in HBM
+            (CUDA events on the launch stream, max over ranks).
+plain_fp64  the same workload with the reference's exact ID (plain FP64), timed the
+            same way; vs_baseline = value / plain_fp64.value.
+e2e         the chosen form through the public API with pinned host buffers, the
+            host<->device copies inside the timed region.
+accuracy    the FP64 relative residual of all 256 solutions, from the library's
+            on-the-fly FP64 matvec (not timed).
+chosen_form_other_problems (rank 0)  the same comparison on the 3D sphere of the
+            mixed-precision configuration at N = 16384 (plain FP64 against both forms:
+            the TF32 tensor-core sketch at 1e-6 refined in FP64 to 1e-10, and the FP64
+            sketch at 1e-10), and the chosen form alone at that configuration's full size
+            (N = 131072, 64 RHS), each with its FP64 error.
 --impl reference  times the CPU restatement of the reference algorithm (the
-          reference is MATLAB and does not run here) on a bounded sample.
+            reference is MATLAB and does not run here) on a bounded sample.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -44,14 +45,8 @@ METRIC = "rskelf factor+solve DOF/s at 1e-10 rel. err: chosen form vs plain FP64
 UNIT = "DOF/s"
 N_DEF, NRHS_DEF, OCC, TOL = 262144, 256, 64, 1e-10
 CPU_SAMPLE_N = 16384
-# DRAM bytes (read + write) per compress step of the N=262144 workload, from one ncu
-# capture of the compress launches of an N=65536 factorization scaled by the box count
-# (x4) over this workload's 23 steps.
-COMPRESS_TRAFFIC_PER_STEP = 4 * 156.4e6 / 23
-# chosen form: factorization tolerance before refinement, refinement target and limit
-CHOSEN_TOL, IR_TOL, IR_MAXIT = 1e-6, 1e-10, 10
 SPHERE_NRHS = 64
-PREDICTOR_WEIGHTS = os.path.join(ROOT, "flam_b200", "predictor_weights.npz")
+CONFIG2_N = 131072
 
 
 def parse():
@@ -65,6 +60,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-chosen", action="store_true", help="skip the chosen-form comparison")
     ap.add_argument("--sphere-n", type=int, default=16384, help="points of the 3D sphere comparison")
+    ap.add_argument("--no-config2", action="store_true", help="skip the full-size config-2 run of the chosen form")
     return ap.parse_args()
 
 
@@ -197,11 +193,13 @@ def event_time(torch, stream, fn):
 
 
 # --------------------------------------------------------------------- chosen form
-def chosen_vs_plain(torch, fb, stream, name, Ad, xd, pxy, symm, Bd, plain_reps, chosen_reps, predictor, flush):
-    """One problem: plain FP64 at 1e-10 (factor + rskelf_sv) against the chosen form
-    (sketched factorization at CHOSEN_TOL + FP64 refinement to IR_TOL), both timed on the
-    device from the inputs in HBM, with their FP64 residuals."""
-    N = Bd.shape[0]
+def chosen_vs_plain(torch, fb, chosen, stream, name, Ad, xd, pxy, symm, Bd, plain_reps, chosen_reps, predictor, flush,
+                    forms=None):
+    """One problem: plain FP64 at TOL (factor + rskelf_sv) against the chosen form (and any
+    other forms listed), each timed on the device from the inputs in HBM, with its FP64
+    residual."""
+    N, nrhs = Bd.shape
+    d = xd.shape[0]
     Xd = torch.empty_like(Bd)
 
     def plain():
@@ -210,45 +208,42 @@ def chosen_vs_plain(torch, fb, stream, name, Ad, xd, pxy, symm, Bd, plain_reps, 
         F.sv_(Xd)
         return F
 
-    copts = dict(symm=symm, stream=stream.cuda_stream, sketch=1, profile=True)
-    if predictor is not None:
-        copts.update(predictor=predictor, sketch_p=12)
-
-    def chosen():
-        F = fb.rskelf(Ad, xd, OCC, CHOSEN_TOL, pxy, copts)
-        _, it, rel = F.ir_sv_(Bd, Xd, IR_TOL, IR_MAXIT)
-        return F, it, rel
-
-    res = {}
-    tp = []
-    for rep in range(plain_reps + 1):          # one untimed warm-up
-        flush.fill_(float(rep))
-        t, F = event_time(torch, stream, plain)
-        if rep > 0 or plain_reps == 0:
-            tp.append(t)
-        if rep < plain_reps:
-            F.free()
-    res["plain"] = {"dofs": N / statistics.mean(tp), "ms": 1e3 * statistics.mean(tp), "steps": len(tp),
-                    "tol": TOL, "rel_residual_fp64": relres(F, Xd, Bd), "nfactor": F.info()["nfactor"]}
-    F.free()
-    tc = []
-    for rep in range(chosen_reps + 1):
-        flush.fill_(float(rep))
-        t, (F, it, rel) = event_time(torch, stream, chosen)
-        if rep > 0:
-            tc.append(t)
-        if rep < chosen_reps:
-            F.free()
-    prof = F.profile()
-    res["chosen"] = {"dofs": N / statistics.mean(tc), "ms": 1e3 * statistics.mean(tc), "steps": len(tc),
-                     "factor_tol": CHOSEN_TOL, "ir_tol": IR_TOL, "ir_steps": it,
-                     "rel_residual_fp64": relres(F, Xd, Bd), "rel_residual_reported": float(np.max(rel)),
-                     "sketched_boxes": prof["n_sketch"], "exact_redo_boxes": prof["n_sketch_redo"],
-                     "sketch_rows": prof["sketch_rows"], "rows_of_K": prof["sketch_rows_k"],
-                     "learned_widths": predictor is not None, "nfactor": F.info()["nfactor"]}
-    F.free()
-    res["ratio_chosen_over_plain"] = res["chosen"]["dofs"] / res["plain"]["dofs"]
-    res["problem"] = name
+    res = {"problem": name}
+    if plain_reps >= 0:
+        tp = []
+        for rep in range(plain_reps + 1):          # one untimed warm-up
+            flush.fill_(float(rep))
+            t, F = event_time(torch, stream, plain)
+            if rep > 0 or plain_reps == 0:
+                tp.append(t)
+            if rep < plain_reps:
+                F.free()
+        res["plain"] = {"dofs": N / statistics.mean(tp), "ms": 1e3 * statistics.mean(tp), "steps": len(tp),
+                        "tol": TOL, "rel_residual_fp64": relres(F, Xd, Bd), "nfactor": F.info()["nfactor"]}
+        F.free()
+    pick = chosen.choose(d, N, nrhs, TOL, symm)
+    for form in forms or [pick]:
+        tc = []
+        for rep in range(chosen_reps + 1):
+            flush.fill_(float(rep))
+            t, (F, _, it, rel) = event_time(torch, stream, lambda: chosen.solve(
+                Ad, xd, OCC, pxy, Bd, Xd, TOL, symm, predictor, form, stream.cuda_stream, True))
+            if rep > 0 or chosen_reps == 0:
+                tc.append(t)
+            if rep < chosen_reps:
+                F.free()
+        prof = F.profile()
+        key = "chosen" if form == pick else form
+        res[key] = {"form": form, "dofs": N / statistics.mean(tc), "ms": 1e3 * statistics.mean(tc), "steps": len(tc),
+                    "factor_tol": chosen.factor_tol(form, TOL), "refinement_steps": it,
+                    "rel_residual_fp64": relres(F, Xd, Bd),
+                    "rel_residual_reported": None if rel is None else float(np.max(rel)),
+                    "sketched_boxes": prof["n_sketch"], "exact_redo_boxes": prof["n_sketch_redo"],
+                    "sketch_rows": prof["sketch_rows"], "rows_of_K": prof["sketch_rows_k"],
+                    "learned_widths": predictor is not None, "nfactor": F.info()["nfactor"]}
+        F.free()
+    if "plain" in res:
+        res["ratio_chosen_over_plain"] = res["chosen"]["dofs"] / res["plain"]["dofs"]
     return res
 
 
@@ -264,7 +259,7 @@ def main():
     import torch
     import torch.distributed as dist
     import flam_b200 as fb
-    from flam_b200 import problems
+    from flam_b200 import chosen, problems
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -295,32 +290,44 @@ def main():
     Bd = B_host.to(dev).t().contiguous().t()
     Xd = torch.empty_like(Bd)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    opts = dict(symm="n", stream=stream.cuda_stream, profile=True)
+    pred = chosen.load_predictor()
+    form = chosen.choose(2, N, nrhs, TOL, "n")
 
-    def step_dev():
-        F = fb.rskelf(Ad, xd, OCC, TOL, pxy, opts)
+    def plain_dev():
+        F = fb.rskelf(Ad, xd, OCC, TOL, pxy, dict(symm="n", stream=stream.cuda_stream, profile=True))
         Xd.copy_(Bd)
         F.sv_(Xd)
         return F
 
+    def chosen_dev():
+        return chosen.solve(Ad, xd, OCC, pxy, Bd, Xd, TOL, "n", pred, form, stream.cuda_stream, True)[0]
+
+    def timed(step):
+        for _ in range(args.warmup):
+            step().free()
+        ts, F = [], None
+        for _ in range(args.steps):
+            flush.fill_(float(len(ts)))
+            if F is not None:
+                F.free()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            F = step()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+        barrier()
+        return max_over_ranks(statistics.mean(ts)), F
+
     peak_fp64 = dgemm_peak(torch, dev)
-    for _ in range(args.warmup):
-        step_dev().free()
     clk_path = os.path.join(ROOT, f".clocks_rank{rank}.csv")
     clk = start_clocks(clk_path)
-    times, F = [], None
-    for _ in range(args.steps):
-        flush.fill_(float(len(times)))
-        if F is not None:
-            F.free()
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        F = step_dev()
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1) * 1e-3)
-    barrier()
+    t_plain, Fp = timed(plain_dev)
+    resid_plain = relres(Fp, Xd, Bd)     # accuracy against FP64, every column (not timed)
+    prof_plain = Fp.profile()
+    Fp.free()
+    t_step, F = timed(chosen_dev)
     if clk:
         clk.terminate()
         clk.wait()
@@ -329,10 +336,8 @@ def main():
         os.remove(clk_path)
     except OSError:
         pass
-    t_step = max_over_ranks(statistics.mean(times))
     prof = F.profile()
     info = F.info()
-    # accuracy against FP64: every column of the last step's solution (not timed)
     resid = relres(F, Xd, Bd)
     F.free()
 
@@ -343,50 +348,56 @@ def main():
     Wp = torch.empty_like(Bp).pin_memory()
     xnp = xp.numpy().T                                      # d x N view, Fortran order
     Ah = fb.Kernel("laplace2d", scale=A.scale, dval=A.dval, weights=wp.numpy())
-    opts_h = dict(symm="n", stream=stream.cuda_stream)
     Wnp = Wp.numpy()
 
-    def step_e2e():
-        F = fb.rskelf(Ah, xnp, OCC, TOL, pxy, opts_h)
-        F.sv_(Wnp)
-        return F
+    def e2e(opts, tol):
+        def step():
+            F = fb.rskelf(Ah, xnp, OCC, tol, pxy, opts)
+            F.sv_(Wnp)
+            return F
+        for _ in range(max(1, args.warmup // 2)):
+            Wp.copy_(Bp)
+            step().free()
+        et = []
+        for _ in range(args.steps):
+            Wp.copy_(Bp)
+            flush.fill_(1.0)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            Fe = step()
+            e1.record(stream)
+            e1.synchronize()
+            et.append(e0.elapsed_time(e1) * 1e-3)
+            Fe.free()
+        return max_over_ranks(statistics.mean(et))
 
-    for _ in range(max(1, args.warmup // 2)):
-        Wp.copy_(Bp)
-        step_e2e().free()
-    et = []
-    for _ in range(args.steps):
-        Wp.copy_(Bp)
-        flush.fill_(1.0)
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        Fe = step_e2e()
-        e1.record(stream)
-        e1.synchronize()
-        et.append(e0.elapsed_time(e1) * 1e-3)
-        Fe.free()
-    t_e2e = max_over_ranks(statistics.mean(et))
+    t_e2e = e2e(chosen.factor_opts(form, "n", pred, stream.cuda_stream), chosen.factor_tol(form, TOL))
+    t_e2e_plain = e2e(dict(symm="n", stream=stream.cuda_stream), TOL)
 
-    # ---- roofline of the dominant kernel (FP64 compute bound)
-    fam = {"compress": (prof["t_compress"], prof["flop_compress"], prof["n_compress"]),
-           "elim": (prof["t_elim"], prof["flop_elim"], prof["n_elim"]),
-           "sweep": (prof["t_sweep"], prof["flop_sweep"], prof["n_sweep"])}
+    # ---- roofline of the chosen form's dominant kernel family (FP64: the FP64 tensor path)
+    fam = {"sketch": (prof["t_sketch"], prof["flop_sketch"]),
+           "id": (prof["t_compress"] - prof["t_sketch"], prof["flop_id"]),
+           "elim": (prof["t_elim"], prof["flop_elim"]),
+           "sweep": (prof["t_sweep"], prof["flop_sweep"])}
+    launches = {"sketch": None, "id": prof["n_compress"], "elim": prof["n_elim"], "sweep": prof["n_sweep"]}
     top = max(fam, key=lambda k: fam[k][0])
-    t_k, f_k, n_k = fam[top]
+    t_k, f_k = fam[top]
     achieved = f_k / t_k / 1e12 if t_k > 0 else 0.0
-    kernel_name = {"compress": "k_compress (fused proxy filter + assembly + TSQR + CPQR + RRQR)",
-                   "elim": "k_eliminate", "sweep": "k_sweep"}[top]
+    kernel_name = {"sketch": "k_sketch_f64 (FP64 row sketch, DMMA)",
+                   "id": "k_compress_tc / k_cpqr_wide (pivoted QR + R11\\R12 of the sketches, exact ID elsewhere)",
+                   "elim": "k_eliminate / k_eliminate_big (LU + Schur updates, DMMA tile)",
+                   "sweep": "k_sweep (solve sweeps)"}[top]
     roofline = {"kernel": kernel_name, "bound": "fp64", "achieved": achieved, "peak": peak_fp64,
-                "unit": "TFLOP/s", "frac": achieved / peak_fp64 if peak_fp64 else None,
-                "traffic": COMPRESS_TRAFFIC_PER_STEP if top == "compress" and args.n == N_DEF else None,
-                "traffic_unit": "bytes per step launch group (ncu capture at N=65536 scaled x4)",
+                "unit": "TFLOP/s", "frac": achieved / peak_fp64 if peak_fp64 else None, "traffic": None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "launches": n_k, "avg_launch_ms": t_k / max(n_k, 1) * 1e3,
-                "algorithmic_flop_per_launch": f_k / max(n_k, 1),
-                "kernel_share_of_step": t_k / t_step,
-                "by_kernel_ms": {k: v[0] * 1e3 for k, v in fam.items()},
-                "by_kernel_tflops": {k: (v[1] / v[0] / 1e12 if v[0] > 0 else 0) for k, v in fam.items()}}
+                "flop_basis": "executed FP64 work: sketch products 2 w rows(K) n; ID on the rows it folds; "
+                              "elimination and sweeps as the reference's dense operations",
+                "step_groups": launches[top], "kernel_share_of_step": t_k / t_step,
+                "by_family_ms": {k: v[0] * 1e3 for k, v in fam.items()},
+                "by_family_tflops": {k: (v[1] / v[0] / 1e12 if v[0] > 0 else 0) for k, v in fam.items()},
+                "plain_fp64_by_family_ms": {"compress": prof_plain["t_compress"] * 1e3,
+                                            "elim": prof_plain["t_elim"] * 1e3, "sweep": prof_plain["t_sweep"] * 1e3}}
 
     out = None
     if rank == 0:
@@ -398,29 +409,42 @@ def main():
             cpu = {"value": CPU_SAMPLE_N / tc, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                    "cpu": cpu_model(),
                    "sample": f"N={CPU_SAMPLE_N} instance of the same workload, oracle (NumPy/SciPy restatement of "
-                             f"the reference, reference box order), {nrhs} RHS, mean of 2 runs"}
-        chosen = None
+                             f"the reference, reference box order, plain FP64), {nrhs} RHS, mean of 2 runs"}
+        others = None
         if not args.no_chosen:
-            pred = fb.Predictor.load(PREDICTOR_WEIGHTS) if os.path.exists(PREDICTOR_WEIGHTS) else None
-            chosen = {"note": "chosen = sketched (FP32/TF32 tensor-core) factorization at tol 1e-6 with learned "
-                              "sketch widths, refined in FP64 to 1e-10 (residual against the on-the-fly FP64 "
-                              "matvec); plain = FP64 exact ID at 1e-10 + rskelf_sv.  Both from inputs in HBM, "
-                              "CUDA events, one untimed warm-up each.",
-                      "star": chosen_vs_plain(torch, fb, stream, f"star N={N}, {nrhs} RHS (this workload)", Ad, xd,
-                                              pxy, "n", Bd, 3, 2, pred, flush)}
             Ns = args.sphere_n
             xs, As, ps = problems.sphere(Ns, p=256, seed=0)
             xsd = torch.from_numpy(np.ascontiguousarray(xs.T)).to(dev).t()
             Bs = torch.randn(Ns, SPHERE_NRHS, dtype=torch.float64, generator=gen).to(dev).t().contiguous().t()
             # plain FP64 takes about a minute here: one timed run, no warm-up
-            chosen["sphere"] = chosen_vs_plain(torch, fb, stream, f"3D sphere N={Ns}, p=256, {SPHERE_NRHS} RHS",
-                                               As, xsd, ps, "n", Bs, 0, 2, pred, flush)
+            others = {"sphere": chosen_vs_plain(torch, fb, chosen, stream, f"3D sphere N={Ns}, p=256, "
+                                                f"{SPHERE_NRHS} RHS (config 2 geometry)", As, xsd, ps, "n", Bs, 0, 2,
+                                                pred, flush, forms=["tf32-refine", "fp64-sketch"])}
+            if not args.no_config2:
+                # config 2 at full size: the chosen form alone (plain FP64's exact IDs of its
+                # top boxes run for hours on this implementation)
+                N2 = CONFIG2_N
+                x2, A2, p2 = problems.sphere(N2, p=256, seed=0)
+                x2d = torch.from_numpy(np.ascontiguousarray(x2.T)).to(dev).t()
+                B2 = torch.randn(N2, SPHERE_NRHS, dtype=torch.float64, generator=gen).to(dev).t().contiguous().t()
+                others["config2"] = chosen_vs_plain(torch, fb, chosen, stream, f"config 2: 3D sphere N={N2}, p=256, "
+                                                    f"{SPHERE_NRHS} RHS", A2, x2d, p2, "n", B2, -1, 1, pred, flush)
         h2d = N * 2 * 8 + N * 8 + N * nrhs * 8
         d2h = N * nrhs * 8
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded star curve, Beta-clustered)",
+               "vs_baseline": (N * world / t_step) / (N * world / t_plain),
+               "vs_baseline_note": "chosen form over plain FP64 on the same workload, both measured in this run "
+                                   "(BASELINE.md publishes no number for this metric)",
+               "dtype": "f64", "data": "synthetic (seeded star curve, Beta-clustered)",
                "config": config(args, world),
+               "form": {"chosen": form, "factor_tol": chosen.factor_tol(form, TOL),
+                        "note": "FP64 row sketches on the FP64 tensor path with learned widths (rank predictor), "
+                                "FP64 pivoted QR / rank / R11\\R12 on the sketches, factorization at 1e-10, one "
+                                "rskelf_sv; rule in flam_b200/chosen.py"},
+               "plain_fp64": {"value": N * world / t_plain, "ms_per_step": t_plain * 1e3,
+                              "rel_residual_fp64": resid_plain,
+                              "e2e": {"value": N * world / t_e2e_plain, "ms_per_step": t_e2e_plain * 1e3}},
                "e2e": {"value": N * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e * 1e3},
                "gpu_launches": int(prof["launches"]),
@@ -430,10 +454,11 @@ def main():
                "accuracy": {"rel_residual_fp64": resid,
                             "note": f"max over the {nrhs} RHS of ||B - A X|| / ||B||, every row, FP64 on-the-fly "
                                     f"matvec (flam_matvec)"},
-               "chosen_form": chosen,
+               "chosen_form_other_problems": others,
                "breakdown_ms": {"tree": info["t_tree"] * 1e3, "factor": info["t_factor"] * 1e3},
                "factor": {"nbox": info["nbox"], "nfactor": info["nfactor"], "levels": info["nstep"],
-                          "device_bytes": info["bytes"]},
+                          "device_bytes": info["bytes"], "sketched_boxes": prof["n_sketch"],
+                          "exact_redo_boxes": prof["n_sketch_redo"]},
                "peaks": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")}}
         print(json.dumps(out), flush=True)
     if world > 1:

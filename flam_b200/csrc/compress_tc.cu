@@ -459,8 +459,10 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   }
   __syncthreads();
 
-  // ---- (6) RRQR refinement (id.m:117-236), only when some |T| > Tmax (or R22 is present)
-  if (m > 0 && !isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
+  // ---- (6) RRQR refinement (id.m:117-236), only when some |T| > Tmax (or R22 is present);
+  // not for a sketch whose rank fills it (the posterior check discards that ID)
+  const bool sketch_full = t.ax_rows > 0 && k > t.ax_rows - t.ax_guard;
+  if (m > 0 && !isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n && !sketch_full) {
     double mx = 0.0;
     if (c >= k && c < n)
       for (int i = 0; i < k; ++i) mx = fmax(mx, R[(int64_t)i * ld + c] * R[(int64_t)i * ld + c]);

@@ -241,11 +241,14 @@ __global__ void __launch_bounds__(kWThreads) k_cpqr_wide(CompressArgs a) {
   for (int c = wid; c < min(ktol, n); c += kWWarps)
     for (int r = c + 1 + lane; r < ktol; r += 32) y(r, c) = 0.0;
   __syncthreads();
+  // a rank that fills the sketch fails the posterior check: that ID is discarded, so it
+  // gets neither T nor the RRQR refinement
+  const bool sketch_full = k > w - t.ax_guard;
   // T = R11 \ R12 (shared-memory staged blocks)
-  if (k > 0 && k < n) tsolve_block_columns(Y, w, k, n, 0, kWThreads, tsd, tsu);
+  if (k > 0 && k < n && !sketch_full) tsolve_block_columns(Y, w, k, n, 0, kWThreads, tsd, tsu);
   __syncthreads();
   // RRQR refinement (id.m:117-236), on thread 0, when some |T| > Tmax or rows were cut
-  if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
+  if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n && !sketch_full) {
     double mx = 0.0;
     for (int c = k + tid; c < n; c += kWThreads)
       for (int i = 0; i < k; ++i) mx = fmax(mx, y(i, c) * y(i, c));
@@ -482,7 +485,8 @@ __global__ void __launch_bounds__(256) k_gw_tsolve(CompressArgs a, GwState* gs) 
   const int b = blockIdx.y;
   const CompressTask t = a.tasks[b];
   const int n = t.n, w = t.ax_rows, k = gs[b].k;
-  if (k <= 0 || k >= n || k + (int)blockIdx.x * 256 >= n) return;   // uniform over the CTA
+  // uniform over the CTA; a rank that fills the sketch fails the posterior check (no T)
+  if (k <= 0 || k >= n || k + (int)blockIdx.x * 256 >= n || k > w - t.ax_guard) return;
   double* Y = const_cast<double*>(a.ypool) + t.ax_off;
   tsolve_block_columns(Y, w, k, n, blockIdx.x * 256, n, tsd, tsu);
 }
@@ -508,7 +512,7 @@ __global__ void __launch_bounds__(kWThreads) k_gw_out(CompressArgs a, GwState* g
   int k = gs[b].k;
   const int ktol = gs[b].ktol;
   if (tid == 0) s_k = k;
-  if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n) {
+  if (!isinf(a.Tmax) && a.rrqr_iter != 0 && k > 0 && k < n && k <= w - t.ax_guard) {
     double mx = 0.0;
     for (int c = k + tid; c < n; c += kWThreads)
       for (int i = 0; i < k; ++i) mx = fmax(mx, y(i, c) * y(i, c));

@@ -214,9 +214,15 @@ def test_fp64_sketch_meets_tight_tolerance_without_refinement(case):
         X = fb.rskelf_sv(F, B)
         res.append((np.linalg.norm(D @ X - B, axis=0) / np.linalg.norm(B, axis=0)).max())
     # the exact ID's residual is tol times the conditioning (Matern with a 1e-2 nugget: ~1e4);
-    # the sketched ID's is within a small factor of it
+    # the sketched ID's is within a small factor of it.  A randomized range finder's error is
+    # bounded by (1 + sqrt(k/(p-1))) s_{k+1} + (e sqrt(k+p)/p) ||s_{k+1:}||_2 (Halko, Martinsson
+    # and Tropp 2011, Thm. 10.6): the second term is the tail's whole energy.  The log kernel
+    # on a curve and the Laplace kernel on a sphere have geometrically decaying tails (that
+    # norm is ~ s_{k+1}); the Matern covariance in a volume has a flat one (~ sqrt(n - k)
+    # s_{k+1}, n - k ~ 100 on this tree), so its factor is allowed to be ten times larger.
+    fac = 100 if case == "matern" else 10
     assert res[0] <= (1e-10 if case != "matern" else 1e-8)
-    assert res[1] <= max(1e-10, 10 * res[0]), res
+    assert res[1] <= max(1e-10, fac * res[0]), res
 
 
 def test_fp64_sketch_with_predicted_widths_and_invalid_option():
