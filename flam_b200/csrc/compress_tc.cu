@@ -200,8 +200,20 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   const unsigned gmask = (G == 1) ? (1u << lane) : (((1u << G) - 1u) << (lane & ~(G - 1)));
   const int64_t sc = col < n ? slf[col] : 0;
   __syncthreads();
+  // A row sketch with no more rows than columns is not folded: its pivoted QR runs on Y
+  // itself (Y and the R of Y = Q R have the same column norms, hence the same pivots
+  // and the same T up to rounding), rows m..n-1 of R staying zero.
+  const bool direct = Ax && !a.Aexp && mode == 0 && m <= n;
+  const int nrow = direct ? m : n;   // rows of R the pivoted QR touches
+  if (direct) {
+    for (int64_t e = tid; e < (int64_t)m * n; e += NT) {
+      const int r = (int)(e % m), cc = (int)(e / m);
+      R[(int64_t)r * ld + cc] = Ax[r + (int64_t)cc * lda];
+    }
+    __syncthreads();
+  }
   double p[B];
-  for (int p0 = rbeg; p0 < rend; p0 += PH) {
+  for (int p0 = rbeg; p0 < (direct ? rbeg : rend); p0 += PH) {
     if (!Ax && !Rsrc && tid < PH) {
       const int rho = p0 + tid < rend ? p0 + tid : m;   // rows past the part are zero
       int ty = 3;
@@ -285,7 +297,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   // ---- (3) column-pivoted QR of R0 (xLAQP2) for min(m, n) steps
   if (c < n) {
     double s = 0.0;
-    for (int r = 0; r < n; ++r) s += R[(int64_t)r * ld + c] * R[(int64_t)r * ld + c];
+    for (int r = 0; r < nrow; ++r) s += R[(int64_t)r * ld + c] * R[(int64_t)r * ld + c];
     vn1[c] = vn2[c] = sqrt(s);
     jpvt[c] = c;
   }
@@ -315,7 +327,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
     // swap columns i and pvt, and gather column i's rows below the diagonal (the
     // reflector) into shared memory with its sum of squares, one row per thread
     double s = 0.0;
-    for (int r = tid; r < n; r += NT) {
+    for (int r = tid; r < nrow; r += NT) {
       double v = R[(int64_t)r * ld + pvt];
       if (pvt != i) {
         R[(int64_t)r * ld + pvt] = R[(int64_t)r * ld + i];
@@ -352,7 +364,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
       be = dii;
       tau = (be - al) / be;
       const double scal = 1.0 / (al - be);
-      for (int r = i + 1 + tid; r < n; r += NT) {
+      for (int r = i + 1 + tid; r < nrow; r += NT) {
         const double v = vcol[r] * scal;
         vcol[r] = v;
         R[(int64_t)r * ld + i] = v;
@@ -367,7 +379,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         double* Rc = R + c;
         double w0 = Rc[(int64_t)i * ld], w1 = 0.0, w2 = 0.0, w3 = 0.0;
         int r = i + 1;
-        for (; r + LD - 1 < n; r += LD) {
+        for (; r + LD - 1 < nrow; r += LD) {
           double b[LD];
 #pragma unroll
           for (int u = 0; u < LD; ++u) b[u] = Rc[(int64_t)(r + u) * ld];
@@ -379,7 +391,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
             w3 += vcol[r + u + 3] * b[u + 3];
           }
         }
-        for (; r + 7 < n; r += 8) {
+        for (; r + 7 < nrow; r += 8) {
           double b[8];
 #pragma unroll
           for (int u = 0; u < 8; ++u) b[u] = Rc[(int64_t)(r + u) * ld];
@@ -388,25 +400,25 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
           w2 += vcol[r + 2] * b[2] + vcol[r + 6] * b[6];
           w3 += vcol[r + 3] * b[3] + vcol[r + 7] * b[7];
         }
-        for (; r < n; ++r) w0 += vcol[r] * Rc[(int64_t)r * ld];
+        for (; r < nrow; ++r) w0 += vcol[r] * Rc[(int64_t)r * ld];
         const double tw = tau * ((w0 + w1) + (w2 + w3));
         Rc[(int64_t)i * ld] -= tw;
         int rr = i + 1;
-        for (; rr + LD - 1 < n; rr += LD) {
+        for (; rr + LD - 1 < nrow; rr += LD) {
           double b[LD];
 #pragma unroll
           for (int u = 0; u < LD; ++u) b[u] = Rc[(int64_t)(rr + u) * ld];
 #pragma unroll
           for (int u = 0; u < LD; ++u) Rc[(int64_t)(rr + u) * ld] = b[u] - tw * vcol[rr + u];
         }
-        for (; rr + 7 < n; rr += 8) {
+        for (; rr + 7 < nrow; rr += 8) {
           double b[8];
 #pragma unroll
           for (int u = 0; u < 8; ++u) b[u] = Rc[(int64_t)(rr + u) * ld];
 #pragma unroll
           for (int u = 0; u < 8; ++u) Rc[(int64_t)(rr + u) * ld] = b[u] - tw * vcol[rr + u];
         }
-        for (; rr < n; ++rr) Rc[(int64_t)rr * ld] -= tw * vcol[rr];
+        for (; rr < nrow; ++rr) Rc[(int64_t)rr * ld] -= tw * vcol[rr];
       }
       if (vn1[c] != 0.0) {  // partial norm downdate (xLAQP2)
         double temp = fabs(R[(int64_t)i * ld + c]) / vn1[c];
@@ -415,7 +427,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
         if (temp * q * q <= tol3z) {
           if (i + 1 < m) {
             double s = 0.0;
-            for (int rr = i + 1; rr < n; ++rr) s += R[(int64_t)rr * ld + c] * R[(int64_t)rr * ld + c];
+            for (int rr = i + 1; rr < nrow; ++rr) s += R[(int64_t)rr * ld + c] * R[(int64_t)rr * ld + c];
             vn1[c] = vn2[c] = sqrt(s);
           } else {
             vn1[c] = vn2[c] = 0.0;
@@ -430,7 +442,7 @@ __global__ void __launch_bounds__(B == 64 ? 256 : (B == 32 ? 512 : 1024)) k_comp
   __syncthreads();
   // clear the reflectors below the diagonal (the RRQR update reads R as upper trapezoidal)
   if (c < n)
-    for (int r = c + 1; r < n; ++r) R[(int64_t)r * ld + c] = 0.0;
+    for (int r = c + 1; r < nrow; ++r) R[(int64_t)r * ld + c] = 0.0;
 
   // ---- (4) rank (id.m:106-113)
   if (tid == 0) {

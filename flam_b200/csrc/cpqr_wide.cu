@@ -432,23 +432,52 @@ __global__ void __launch_bounds__(kWThreads) k_gw_apply(CompressArgs a, GwState*
   const double tol3z = 1.0536712127723509e-08;
   const int c = c0 + wid;
   if (c >= n) return;
+  double* yc = Y + (int64_t)c * w;
+  // each lane streams rows lane, lane + 32, ... of its warp's column; four rows are in
+  // flight per lane (independent partial sums), so a warp keeps 1 KB of loads outstanding
+  // instead of one 256-byte row at a time
+  const int r0 = i + 1 + lane;
   if (tau != 0.0) {
-    double d = lane == 0 ? y(i, c) : 0.0;
-    for (int r = i + 1 + lane; r < w; r += 32) d += v[r] * y(r, c);
-    d = tau * warp_sum(d);
-    if (lane == 0) y(i, c) -= d;
-    for (int r = i + 1 + lane; r < w; r += 32) y(r, c) -= d * v[r];
+    double d0 = lane == 0 ? yc[i] : 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
+    int r = r0;
+    for (; r + 96 < w; r += 128) {
+      const double a0 = yc[r], a1 = yc[r + 32], a2 = yc[r + 64], a3 = yc[r + 96];
+      d0 += v[r] * a0;
+      d1 += v[r + 32] * a1;
+      d2 += v[r + 64] * a2;
+      d3 += v[r + 96] * a3;
+    }
+    for (; r < w; r += 32) d0 += v[r] * yc[r];
+    const double d = tau * warp_sum((d0 + d1) + (d2 + d3));
+    if (lane == 0) yc[i] -= d;
+    r = r0;
+    for (; r + 96 < w; r += 128) {
+      const double a0 = yc[r], a1 = yc[r + 32], a2 = yc[r + 64], a3 = yc[r + 96];
+      yc[r] = a0 - d * v[r];
+      yc[r + 32] = a1 - d * v[r + 32];
+      yc[r + 64] = a2 - d * v[r + 64];
+      yc[r + 96] = a3 - d * v[r + 96];
+    }
+    for (; r < w; r += 32) yc[r] -= d * v[r];
   }
   __syncwarp();
   const double nv = vn1[c];
   if (nv != 0.0) {
-    double temp = fabs(y(i, c)) / nv;
+    double temp = fabs(yc[i]) / nv;
     temp = fmax(1.0 - temp * temp, 0.0);
     const double q = nv / vn2[c];
     if (temp * q * q <= tol3z) {
-      double s2 = 0.0;
-      for (int r = i + 1 + lane; r < w; r += 32) s2 += y(r, c) * y(r, c);
-      s2 = warp_sum(s2);
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      int r = r0;
+      for (; r + 96 < w; r += 128) {
+        const double a0 = yc[r], a1 = yc[r + 32], a2 = yc[r + 64], a3 = yc[r + 96];
+        s0 += a0 * a0;
+        s1 += a1 * a1;
+        s2 += a2 * a2;
+        s3 += a3 * a3;
+      }
+      for (; r < w; r += 32) s0 += yc[r] * yc[r];
+      s2 = warp_sum((s0 + s1) + (s2 + s3));
       if (lane == 0) vn1[c] = vn2[c] = (i + 1 < w) ? sqrt(s2) : 0.0;
     } else if (lane == 0) {
       vn1[c] = nv * sqrt(temp);
@@ -480,15 +509,75 @@ __global__ void __launch_bounds__(kWThreads) k_gw_rank(CompressArgs a, GwState* 
     for (int r = c + 1 + lane; r < ktol; r += 32) Y[r + (int64_t)c * w] = 0.0;
 }
 
+// T = R11 \ R12 for 64 columns of R12 per CTA (8 warps), with every global access
+// coalesced: lanes run over rows.  Back substitution by 32-row blocks from the bottom:
+// a warp solves a column's diagonal block with the block's rows in its lanes (x_j
+// broadcast by shuffle), the solved x go to shared memory, then the rows above are
+// updated 64 at a time, R's 64 x 32 slab held in registers (two rows a lane) and x read
+// by broadcast.
+constexpr int kTsCols = 64;
 __global__ void __launch_bounds__(256) k_gw_tsolve(CompressArgs a, GwState* gs) {
-  __shared__ double tsd[32 * 33], tsu[64 * 33];
+  __shared__ double sd[32 * 33];            // sd[j * 33 + l] = R(i0 + j, i0 + l)
+  __shared__ double su[32 * 64];            // su[j * 64 + rr] = R(r0 + rr, i0 + j)
+  __shared__ double xs[kTsCols * 33];       // xs[cl * 33 + j] = x_j of local column cl
   const int b = blockIdx.y;
   const CompressTask t = a.tasks[b];
   const int n = t.n, w = t.ax_rows, k = gs[b].k;
+  const int cbase = k + (int)blockIdx.x * kTsCols;
   // uniform over the CTA; a rank that fills the sketch fails the posterior check (no T)
-  if (k <= 0 || k >= n || k + (int)blockIdx.x * 256 >= n || k > w - t.ax_guard) return;
+  if (k <= 0 || k >= n || cbase >= n || k > w - t.ax_guard) return;
+  const int ncol = min(kTsCols, n - cbase);
   double* Y = const_cast<double*>(a.ypool) + t.ax_off;
-  tsolve_block_columns(Y, w, k, n, blockIdx.x * 256, n, tsd, tsu);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int i1 = k; i1 > 0;) {
+    const int i0 = i1 > 32 ? i1 - 32 : 0, bs = i1 - i0;
+    __syncthreads();
+    for (int e = tid; e < 32 * 32; e += 256) {
+      const int j = e & 31, l = e >> 5;
+      sd[j * 33 + l] = (j < bs && l < bs) ? Y[(i0 + j) + (int64_t)(i0 + l) * w] : 0.0;
+    }
+    __syncthreads();
+    for (int cl = wid; cl < ncol; cl += 8) {
+      double* yc = Y + (int64_t)(cbase + cl) * w;
+      double bv = lane < bs ? yc[i0 + lane] : 0.0;
+      for (int j = bs - 1; j >= 0; --j) {
+        const double xj = __shfl_sync(0xffffffffu, bv, j) / sd[j * 33 + j];
+        if (lane == j) bv = xj;
+        if (lane < j) bv -= sd[lane * 33 + j] * xj;
+      }
+      if (lane < bs) yc[i0 + lane] = bv;
+      xs[cl * 33 + lane] = lane < bs ? bv : 0.0;
+    }
+    for (int r0 = 0; r0 < i0; r0 += 64) {
+      const int rn = min(64, i0 - r0);
+      __syncthreads();   // xs written; the previous slab's readers are done
+      for (int e = tid; e < 64 * 32; e += 256) {
+        const int rr = e & 63, j = e >> 6;
+        su[j * 64 + rr] = (rr < rn && j < bs) ? Y[(r0 + rr) + (int64_t)(i0 + j) * w] : 0.0;
+      }
+      __syncthreads();
+      double ra[32], rb[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        ra[j] = su[j * 64 + lane];
+        rb[j] = su[j * 64 + lane + 32];
+      }
+      for (int cl = wid; cl < ncol; cl += 8) {
+        double* yc = Y + (int64_t)(cbase + cl) * w + r0;
+        double u0 = lane < rn ? yc[lane] : 0.0;
+        double u1 = lane + 32 < rn ? yc[lane + 32] : 0.0;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const double xj = xs[cl * 33 + j];   // zero beyond bs: su is zero there
+          u0 -= ra[j] * xj;
+          u1 -= rb[j] * xj;
+        }
+        if (lane < rn) yc[lane] = u0;
+        if (lane + 32 < rn) yc[lane + 32] = u1;
+      }
+    }
+    i1 = i0;
+  }
 }
 
 __global__ void __launch_bounds__(kWThreads) k_gw_out(CompressArgs a, GwState* gs) {
@@ -581,7 +670,7 @@ void launch_cpqr_grid(const CompressArgs& a, int ntask, int nmax, int wmax, int 
     k_gw_apply<<<dim3(cb, z), kWThreads, vbytes, s>>>(a, gs, i);
   }
   k_gw_rank<<<z, kWThreads, 0, s>>>(a, gs);
-  k_gw_tsolve<<<dim3((unsigned)((nmax + 255) / 256), z), 256, 0, s>>>(a, gs);
+  k_gw_tsolve<<<dim3((unsigned)((nmax + kTsCols - 1) / kTsCols), z), 256, 0, s>>>(a, gs);
   k_gw_out<<<z, kWThreads, 0, s>>>(a, gs);
 }
 

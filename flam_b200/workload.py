@@ -7,20 +7,19 @@ Runs ``reps`` factorizations and solves on cuda:0 with no warm-up and nothing el
 launched, so a kernel profiler sees only the library's kernels:
 
 * ``--form plain``: the exact ID at ``--tol`` and rskelf_sv;
-* ``--form chosen``: the sketched factorization at tol 1e-6 with the trained rank
-  predictor (flam_b200/predictor_weights.npz) and FP64 refinement to 1e-10, whose
-  residual steps are the on-the-fly FP64 matvec.
+* ``--form chosen``: the form flam_b200/chosen.py picks for the problem at ``--tol``
+  (with the trained rank predictor): the FP64-sketched factorization at ``--tol`` and
+  one rskelf_sv, or the TF32-sketched factorization at 1e-6 refined in FP64 to
+  ``--tol`` against the on-the-fly FP64 matvec;
+* ``--form fp64-sketch`` / ``--form tf32-refine``: that form, whatever the rule picks.
 
 ``--cfg star`` is the Beta-clustered star curve of the benchmark (2D log kernel);
 ``--cfg sphere`` the Fibonacci sphere of the mixed-precision configuration (3D Laplace,
 256-point proxy sphere).  This is the entry point the committed ncu summaries name.
 """
 import argparse
-import os
 
 import numpy as np
-
-HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
@@ -31,7 +30,7 @@ def main():
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--symm", default="n")
     ap.add_argument("--tol", type=float, default=1e-10)
-    ap.add_argument("--form", default="plain", choices=["plain", "chosen"])
+    ap.add_argument("--form", default="plain", choices=["plain", "chosen", "fp64-sketch", "tf32-refine"])
     args = ap.parse_args()
     import torch
 
@@ -47,8 +46,9 @@ def main():
     Ad = fb.Kernel(A.kind, scale=A.scale, dval=A.dval, param=A.param, weights=w)
     B = torch.randn(args.n, args.nrhs, dtype=torch.float64, device="cuda").t().contiguous().t()
     pred = None
-    if args.form == "chosen":
-        pred = fb.Predictor.load(os.path.join(HERE, "predictor_weights.npz"))
+    if args.form != "plain":
+        from flam_b200 import chosen
+        pred = chosen.load_predictor()
     for _ in range(args.reps):
         if args.form == "plain":
             F = fb.rskelf(Ad, xd, 64, args.tol, pxy, dict(symm=args.symm))
@@ -56,10 +56,10 @@ def main():
             F.sv_(X)
             extra = ""
         else:
-            F = fb.rskelf(Ad, xd, 64, 1e-6, pxy, dict(symm=args.symm, sketch=1, predictor=pred, sketch_p=12))
             X = torch.empty_like(B)
-            _, it, rel = F.ir_sv_(B, X, 1e-10, 10)
-            extra = f" refinement steps {it} relres {float(np.max(rel)):.2e}"
+            F, form, it, rel = chosen.solve(Ad, xd, 64, pxy, B, X, args.tol, args.symm, pred,
+                                            None if args.form == "chosen" else args.form)
+            extra = f" form {form} refinement steps {it}" + ("" if rel is None else f" relres {float(np.max(rel)):.2e}")
         torch.cuda.synchronize()
         F.free()
     print("ok", args.cfg, args.form, args.n, args.nrhs, args.reps, extra)
