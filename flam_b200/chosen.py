@@ -34,6 +34,7 @@ REFINE_MAX_ITER = 10
 # refinement only while N * nrhs stays at most this (two residual products of
 # 2 N^2 nrhs flop each take well under a second on the FP64 tensor path)
 REFINE_MAX_N_NRHS = 1 << 23
+NOT_SPD = 2   # FLAM_ERR_NOT_SPD (FLAM:rskelf:notPosDef)
 
 
 def choose(d, N, nrhs, tol, symm="n"):
@@ -71,14 +72,27 @@ def solve(A, x, occ, pxyfun, B, X, tol=1e-10, symm="n", predictor=None, form=Non
     """Factor A on points x in the chosen form and solve A X = B to relative residual tol.
 
     B and X are device tensors (N x nrhs, column-major); X is overwritten.  Returns
-    (F, form, refinement steps, per-column relative residual or None).  The residual is
+    (F, form, refinement steps, per-column relative residual or None).  With symm 'p', a
+    sketched factorization that fails the positive-definite check of a redundant block is
+    redone with symm 'n' (LU of the same matrix); ``F.symm`` tells which ran.  The residual is
     measured by the refinement itself in the "tf32-refine" form; the "fp64-sketch" form
     computes none (check it with ``F.matvec_``)."""
     d, N = int(x.shape[0]), int(x.shape[1])
     nrhs = int(B.shape[1]) if B.ndim == 2 else 1
     form = form or choose(d, N, nrhs, tol, symm)
+    from ._lib import FlamError
     from .api import rskelf
-    F = rskelf(A, x, occ, factor_tol(form, tol), pxyfun, factor_opts(form, symm, predictor, stream, profile))
+    try:
+        F = rskelf(A, x, occ, factor_tol(form, tol), pxyfun, factor_opts(form, symm, predictor, stream, profile))
+    except FlamError as e:
+        if symm != "p" or e.code != NOT_SPD:
+            raise
+        # The exact ID keeps every Schur complement of an SPD matrix SPD; a sketched ID's
+        # interpolation error can leave a redundant block indefinite at the level of the
+        # tolerance (seen on Matern covariances whose ranks fill the sketch).  The form
+        # then factors the same symmetric matrix with LU (symm 'n').
+        symm = "n"
+        F = rskelf(A, x, occ, factor_tol(form, tol), pxyfun, factor_opts(form, symm, predictor, stream, profile))
     if form == "tf32-refine":
         _, it, rel = F.ir_sv_(B, X, tol, max_iter)
         return F, form, it, np.asarray(rel)
