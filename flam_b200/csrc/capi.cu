@@ -953,6 +953,14 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     }
   }
 
+  // global compression (no proxy function): the leaf boxes of each instance
+  bool any_global = false;
+  for (int i = 0; i < ninst; ++i) any_global |= F.iph[i].pkind == P_NONE;
+  std::vector<std::vector<int32_t>> leaves(any_global ? ninst : 0);
+  if (any_global)
+    for (int64_t b = 0; b < nbox; ++b)
+      if (F.nch[b] == 0 && F.iph[F.binst[b]].pkind == P_NONE) leaves[F.binst[b]].push_back((int32_t)b);
+
   std::vector<int64_t> xoff(nbox), xlen(nbox), Moff(nbox, -1);
   for (int64_t b = 0; b < nbox; ++b) {
     const bool leaf = F.nch[b] == 0;
@@ -1082,14 +1090,41 @@ void factorize(flam_factor& F, double rank_or_tol, const flam_opts& o) {
     if (top > F.ipool.cap) ws.wait_elim(s, par ^ 1);   // growth frees the pool the last elimination reads
     F.ipool.reserve(top, s);
     F.ipool.n = top;
-    // ---- neighbour candidates: current xi of every neighbour (rskelf.m:186)
+    // ---- neighbour candidates: current xi of every neighbour (rskelf.m:186).  Without a
+    // proxy function a box below level 2 is compressed against every remaining point of
+    // its instance instead (rskelf.m:204, nbr = setdiff(find(rem), slf)): the other boxes
+    // of this level after the pull-up, and the leaves of coarser levels (not yet reached).
     std::vector<CopySeg> cs;
     std::vector<int64_t> cand_off(nb), ncand(nb);
+    std::vector<std::vector<int>> inst_q;   // global compression: this step's boxes per instance
+    if (any_global) {
+      inst_q.resize(ninst);
+      for (int q = 0; q < nb; ++q) inst_q[F.binst[boxes[q]]].push_back(q);
+    }
     int64_t ctop = 0;
     for (int q = 0; q < nb; ++q) {
       const int32_t b = boxes[q];
       cand_off[q] = ctop;
       int64_t n = 0;
+      const int ib = F.binst[b];
+      if (F.iph[ib].pkind == P_NONE && F.depth[b] > 2) {
+        for (int q2 : inst_q[ib])
+          if (q2 != q && nslf[q2] > 0) {
+            cs.push_back(CopySeg{slf_off[q2], ctop + n, nslf[q2]});
+            n += nslf[q2];
+          }
+        for (int32_t j : leaves[ib])
+          if (F.depth[j] < F.depth[b] && xlen[j] > 0) {
+            cs.push_back(CopySeg{xoff[j], ctop + n, xlen[j]});
+            n += xlen[j];
+          }
+        if (n > INT32_MAX / 2)
+          fail(FLAM_ERR_ARG, "FLAM:gpu:globalTooLarge: global compression of a box against %lld points exceeds "
+                             "the device limit", (long long)n);
+        ncand[q] = n;
+        ctop += n;
+        continue;
+      }
       for (int64_t e = F.nbor_ptr[b]; e < F.nbor_ptr[b + 1]; ++e) {
         const int32_t j = F.nbor[e];
         int64_t so, sl;
@@ -1990,16 +2025,16 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
   px.kind = FLAM_PROXY_NONE;
   if (pxy) px = *pxy;
   if (px.kind < 0 || px.kind > 3) fail(FLAM_ERR_ARG, "FLAM:gpu:unsupportedProxy: unknown proxy kind %d", px.kind);
-  if (px.kind == FLAM_PROXY_NONE)
-    fail(FLAM_ERR_UNSUPPORTED,
-         "FLAM:gpu:unsupportedHandle: rskelf without a proxy (global compression) is not available on the device");
-  if (px.kind == FLAM_PROXY_RING && d != 2) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: ring proxy needs d = 2");
-  if (px.kind == FLAM_PROXY_SPHERE && d != 3) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: sphere proxy needs d = 3");
-  if (px.p < 1) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: proxy needs p >= 1 points");
-  if (px.kind == FLAM_PROXY_ANNULUS && (px.p_rad < 1 || !(px.param > 0)))
-    fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: annulus proxy needs p_rad >= 1 and param > 0");
-  if (px.kernel_kind < 0 || px.kernel_kind > 4 || px.kernel_kind == FLAM_KERNEL_LAPLACE2D_DL)
-    fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: proxy kernel must be a single-layer registry kernel");
+  // px.kind == FLAM_PROXY_NONE: global compression (rskelf.m:204), nothing more to check
+  if (px.kind != FLAM_PROXY_NONE) {
+    if (px.kind == FLAM_PROXY_RING && d != 2) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: ring proxy needs d = 2");
+    if (px.kind == FLAM_PROXY_SPHERE && d != 3) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: sphere proxy needs d = 3");
+    if (px.p < 1) fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: proxy needs p >= 1 points");
+    if (px.kind == FLAM_PROXY_ANNULUS && (px.p_rad < 1 || !(px.param > 0)))
+      fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: annulus proxy needs p_rad >= 1 and param > 0");
+    if (px.kernel_kind < 0 || px.kernel_kind > 4 || px.kernel_kind == FLAM_KERNEL_LAPLACE2D_DL)
+      fail(FLAM_ERR_ARG, "FLAM:gpu:invalidProxy: proxy kernel must be a single-layer registry kernel");
+  }
   bool any_w = false, any_n = false;
   for (int i = 0; i < ninst; ++i) {
     if (N[i] < 1) fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidArg: every instance needs N >= 1");

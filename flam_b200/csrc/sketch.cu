@@ -391,13 +391,16 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch_f64(SketchArgs a) {
   const int m = nrep * m1 + npr;
   if (tid == 0) a.mrows[t.out_idx] = m;
   const int64_t* cand = a.cpool + t.cand_off;
-  // entry (rho, columns cg * 8 .. + 7) of each chunk for this thread
+  // entries (rho, columns cg * cpt .. + cpt - 1) of each chunk for this thread: a tile of
+  // at most half the columns spreads them over every thread (cpt = 4), not half of them
+  constexpr int kCpt = kSketchF64Cols / (kSkThreads / kFk);
+  const int cpt = n <= kSketchF64Cols / 2 ? kCpt / 2 : kCpt;
   const int rho_t = tid & (kFk - 1), cg = tid / kFk;
-  int64_t scol[kSketchF64Cols / (kSkThreads / kFk)];
+  int64_t scol[kCpt];
 #pragma unroll
-  for (int i = 0; i < kSketchF64Cols / (kSkThreads / kFk); ++i) {
-    const int c = cg * (kSketchF64Cols / (kSkThreads / kFk)) + i;
-    scol[i] = c < n ? a.ipool[t.slf_off + t.col0 + c] : -1;
+  for (int i = 0; i < kCpt; ++i) {
+    const int c = cg * cpt + i;
+    scol[i] = (i < cpt && c < n) ? a.ipool[t.slf_off + t.col0 + c] : -1;
   }
   double acc[4][4][2];
 #pragma unroll
@@ -436,10 +439,10 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch_f64(SketchArgs a) {
     {
       const RowDescF& rd = rows[rho_t];
 #pragma unroll
-      for (int i = 0; i < kSketchF64Cols / (kSkThreads / kFk); ++i) {
-        const int c = cg * (kSketchF64Cols / (kSkThreads / kFk)) + i;
-        Ks[c * kFld + rho_t] =
-            scol[i] >= 0 && rd.type != 3 ? block_entry(P, ip, rd.type, rd.q, rd.y, rd.wmul, scol[i]) : 0.0;
+      for (int i = 0; i < kCpt; ++i) {
+        if (i < cpt)
+          Ks[(cg * cpt + i) * kFld + rho_t] =
+              scol[i] >= 0 && rd.type != 3 ? block_entry(P, ip, rd.type, rd.q, rd.y, rd.wmul, scol[i]) : 0.0;
       }
     }
     for (int e = tid; e < kSketchF64Rows * kFk; e += kSkThreads) {
@@ -447,7 +450,9 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch_f64(SketchArgs a) {
       Os[j * kFld + rr] = (j < w && rho < m) ? (double)omega(a.seed, t.box, rho, t.j0 + j) : 0.0;
     }
     __syncthreads();
-    if (wj * 32 < w) {
+    // warps whose 32 x 32 block lies beyond the tile's rows or columns have no products
+    // (with cpt = 4, Ks holds only columns below 64)
+    if (wj * 32 < w && wc * 32 < n) {
       const double* Aw = Os + (wj * 32 + g) * kFld + tq;
       const double* Bw = Ks + (wc * 32 + g) * kFld + tq;
 #pragma unroll

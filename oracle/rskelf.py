@@ -114,6 +114,9 @@ def rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None, order="reference", tr
         for i in boxes:                                            # rskelf.m:179-181
             xi[i] = np.concatenate([xi[i]] + [xi[c] for c in t["chld"][i]]).astype(np.int64)
         snap = [a for a in xi] if order == "level_sync" else None
+        # global compression (no pxyfun) sees the points remaining when the level starts in
+        # the level-synchronous order, and rem as each box leaves it in the reference's
+        rem_nbr = rem.copy() if order == "level_sync" else rem
         for i in boxes:
             slf = xi[i]
             src = snap if snap is not None else xi
@@ -133,7 +136,7 @@ def rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None, order="reference", tr
             Kpxy = np.zeros((0, nslf))
             if lvl > 2:                                            # rskelf.m:203-207
                 if pxyfun is None:
-                    nbr = np.setdiff1d(np.flatnonzero(rem), slf)
+                    nbr = np.setdiff1d(np.flatnonzero(rem_nbr), slf)
                 else:
                     Kpxy, nbr = pxyfun(x, slf, nbr, l, t["ctr"][i])
             K = A(nbr, slf)                                        # rskelf.m:210-212
