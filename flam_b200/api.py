@@ -354,9 +354,35 @@ def _points(x):
     return a.ctypes.data, a.shape[0], a.shape[1], a
 
 
+def _stop_levels(stop, x, occ, opts):
+    """Levels an ``opts.stop`` predicate lets the factorization run (rskelf.m:128,172).
+
+    The reference calls ``stop(nlvl - lvl, l)`` before each level (``l`` the level's box
+    size, d values) and stops at the first true.  The levels and their sizes come from the
+    tree alone, so the predicate is evaluated here on the tree rskelf builds (same occ,
+    lvlmax and ext) and the library gets the equivalent level count."""
+    if _is_cuda_tensor(x):
+        x = x.detach().cpu().numpy()
+    T = hypoct(x, occ, (opts or {}).get("lvlmax", math.inf), (opts or {}).get("ext"))
+    try:
+        t = T.tree()
+    finally:
+        T.free()
+    nlvl, l = t["nlvl"], np.asarray(t["l"])
+    for done in range(nlvl):
+        if stop(done, l[:, nlvl - done - 1].copy()):
+            return done
+    return math.inf
+
+
 def rskelf(A, x, occ, rank_or_tol, pxyfun=None, opts=None):
-    """F = rskelf(A, x, occ, rank_or_tol, pxyfun, opts)   rskelf/rskelf.m:109-309."""
+    """F = rskelf(A, x, occ, rank_or_tol, pxyfun, opts)   rskelf/rskelf.m:109-309.
+
+    ``opts["stop"]`` is a level count or, as in the reference, a predicate
+    ``stop(levels_done, l)``."""
     _check_handles(A, pxyfun)
+    if opts and callable(opts.get("stop")):
+        opts = dict(opts, stop=_stop_levels(opts["stop"], x, occ, opts))
     ptr, d, N, keep_x = _points(x)
     o, keep = _c_opts(opts)
     ka = A.c_struct()
@@ -372,6 +398,9 @@ def rskelf_batched(As, xs, occ, rank_or_tol, pxyfun=None, opts=None, sizes=None)
 
     ``xs`` is a list of d x N_i point arrays, or (with ``sizes``) one d x sum(N_i)
     column-major CUDA tensor of all instances' points, used in place."""
+    if opts and callable(opts.get("stop")):
+        raise _lib.FlamError(1, "FLAM:rskelf:invalidArg: a stop predicate needs one problem (each instance has its "
+                                "own tree); pass a level count")
     for A in As:
         _check_handles(A, pxyfun)
     if sizes is not None:
