@@ -15,6 +15,7 @@ STATUS = {
     0: "FLAM_OK", 1: "FLAM_ERR_ARG", 2: "FLAM_ERR_NOT_SPD", 3: "FLAM_ERR_CUDA", 4: "FLAM_ERR_NOMEM",
     5: "FLAM_ERR_UNSUPPORTED", 6: "FLAM_ERR_TIMEOUT",
     100: "FLAM_WARN_RRQR_MAXITER", 101: "FLAM_WARN_SINGULAR", 102: "FLAM_WARN_IR_NOT_CONVERGED",
+    103: "FLAM_WARN_LDL_AS_LU",
 }
 
 # every symbol include/flam.h declares

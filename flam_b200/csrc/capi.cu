@@ -2016,11 +2016,14 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
   if (!(occ >= 0)) fail(FLAM_ERR_ARG, "FLAM:hypoct:invalidOcc: Leaf occupancy must be nonnegative.");
   if (!(rank_or_tol >= 0)) fail(FLAM_ERR_ARG, "FLAM:id:invalidRankOrTol: Rank or tolerance must be nonnegative.");
   if (!(o.Tmax >= 1)) fail(FLAM_ERR_ARG, "FLAM:id:invalidTmax: Interpolation matrix entry bound must be >= 1.");
-  const char symm = chksymm(o.symm);
+  char symm = chksymm(o.symm);
   if (o.sketch < 0 || o.sketch > 2)
     fail(FLAM_ERR_ARG, "FLAM:rskelf:invalidSketch: opts.sketch must be 0 (exact ID), 1 (TF32 sketch) or 2 (FP64 sketch)");
-  if (symm == 'h')
-    fail(FLAM_ERR_UNSUPPORTED, "FLAM:gpu:unsupportedSymm: symm 'h' (LDL) is not available on the device path");
+  // symm 'h' (LDL of the redundant blocks, rskelf.m:229): there is no LDL on the device, so
+  // the factorization takes LU ('n') and warns, as the reference does under Octave
+  // (rskelf.m:124-127, FLAM:rskelf:octaveLDL)
+  const bool ldl_as_lu = symm == 'h';
+  if (ldl_as_lu) symm = 'n';
   flam_proxy px{};
   px.kind = FLAM_PROXY_NONE;
   if (pxy) px = *pxy;
@@ -2136,6 +2139,10 @@ flam_status create(int ninst, const double* x, int d, const int64_t* N, const fl
   if ((*out)->warn & 2) {
     g_err = "FLAM:rskelf:singular: an LU pivot of a redundant block was exactly zero";
     return FLAM_WARN_SINGULAR;
+  }
+  if (ldl_as_lu) {
+    g_err = "FLAM:rskelf:octaveLDL: No LDL decomposition on the device; using LU.";
+    return FLAM_WARN_LDL_AS_LU;
   }
   return FLAM_OK;
 }

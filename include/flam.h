@@ -52,7 +52,8 @@ typedef enum {
   FLAM_ERR_TIMEOUT = 6,      /* a bounded device wait gave up (the sketch kernel's mbarrier) */
   FLAM_WARN_RRQR_MAXITER = 100, /* FLAM:id:maxIterCount (factor is still valid) */
   FLAM_WARN_SINGULAR = 101,     /* an LU pivot of a redundant block was exactly zero */
-  FLAM_WARN_IR_NOT_CONVERGED = 102 /* refinement stopped above ir_tol (X is the last iterate) */
+  FLAM_WARN_IR_NOT_CONVERGED = 102, /* refinement stopped above ir_tol (X is the last iterate) */
+  FLAM_WARN_LDL_AS_LU = 103         /* symm 'h' factored with LU, FLAM:rskelf:octaveLDL (rskelf.m:124-127) */
 } flam_status;
 
 /* Kernel registry: the matrix entry is A(i,j) = scale * w_j * K(x_i, x_j) for

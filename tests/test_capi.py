@@ -55,9 +55,6 @@ def test_bad_arguments_fail_before_the_device():
         fb.rskelf(lambda i, j: np.zeros((len(i), len(j))), x, 64, 1e-10, pxy)
     assert e.value.identifier == "FLAM:gpu:unsupportedHandle"
     with pytest.raises(fb.FlamError) as e:
-        fb.rskelf(A, x, 64, 1e-10, pxy, dict(symm="h"))
-    assert e.value.identifier == "FLAM:gpu:unsupportedSymm"
-    with pytest.raises(fb.FlamError) as e:
         fb.Kernel("helmholtz")
     assert e.value.identifier == "FLAM:gpu:unsupportedKernel"
     with pytest.raises(fb.FlamError) as e:
