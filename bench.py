@@ -20,6 +20,7 @@ e2e         the chosen form through the public API with pinned host buffers, the
             host<->device copies inside the timed region.
 accuracy    the FP64 relative residual of all 256 solutions, from the library's
             on-the-fly FP64 matvec (not timed).
+value_excluding_tree  `value` with the tree construction's device time taken out.
 chosen_form_other_problems (rank 0)  the same comparison on the 3D sphere of the
             mixed-precision configuration at N = 16384 (plain FP64 against both forms:
             the TF32 tensor-core sketch at 1e-6 refined in FP64 to 1e-10, and the FP64
@@ -456,6 +457,7 @@ def main():
                                     f"matvec (flam_matvec)"},
                "chosen_form_other_problems": others,
                "breakdown_ms": {"tree": info["t_tree"] * 1e3, "factor": info["t_factor"] * 1e3},
+               "value_excluding_tree": N * world / max(t_step - info["t_tree"], 1e-9),
                "factor": {"nbox": info["nbox"], "nfactor": info["nfactor"], "levels": info["nstep"],
                           "device_bytes": info["bytes"], "sketched_boxes": prof["n_sketch"],
                           "exact_redo_boxes": prof["n_sketch_redo"]},
