@@ -106,9 +106,9 @@ typedef struct {
   /* Sketched (mixed-precision) compression -- not in the reference.  0: the reference's
    * ID of the full block K (id.m).  1: the ID of a row sketch Y = Omega K (Omega w x m,
    * +-1 entries) formed in FP32 on the tensor cores (K split into two TF32 parts),
-   * with the FP64 pivoted QR, rank and R11 \ R12 on Y; boxes of more than 256 points use
-   * the exact ID.  A box whose rank comes within sketch_guard of w is redone exactly
-   * (the posterior check).  Meant for loose tolerances (>= ~1e-7: the sketch carries
+   * with the FP64 pivoted QR, rank and R11 \ R12 on Y; boxes of more than 8192 points
+   * use the exact ID.  A box whose rank comes within sketch_guard of w is redone with a
+   * second sketch at full width, or exactly when that fills too (the posterior check).  Meant for loose tolerances (>= ~1e-7: the sketch carries
    * ~21 bits) followed by flam_rskelf_ir_sv.  2: the same sketched ID with K's entries and
    * the products in FP64 (FP64 tensor path), for tight tolerances without refinement.
    * Other values: FLAM_ERR_ARG (FLAM:rskelf:invalidSketch). */
